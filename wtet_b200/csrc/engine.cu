@@ -1,0 +1,1579 @@
+// B200 Delaunay engine: parallel Bowyer-Watson cavity insertion with exact
+// FP64 predicates and Simulation of Simplicity.
+//
+// What it replaces in half-potato/wtet: the phase-1 GPU loop (src/phase1.rs,
+// src/gpu/*.rs, src/shaders/*.wgsl: vote, split, flip, relocate, compact) and
+// the phase-2 host repair (src/phase2.rs, src/cpu/*).  Each insertion round
+// keeps the triangulation exactly Delaunay: a point replaces the cavity of
+// tets whose circumsphere contains it (the reference's own exact criterion,
+// src/phase2.rs:428-470) by the star of the cavity boundary; concurrent
+// insertions are admitted only when their cavities are disjoint and no cavity
+// touches another's ring of neighbouring tets, which makes every round
+// equivalent to some sequential order.  The result is therefore the unique
+// SoS Delaunay triangulation, with no flip failures and nothing left to repair.
+//
+// Round structure (one insertion round over all clouds of a job):
+//   k_vote        each uninserted point votes for its tet (64-bit atomicMax of
+//                 score | ~point, src/shaders/vote.wgsl semantics)
+//   k_expand      each vote winner grows its cavity by BFS with exact insphere,
+//                 claiming cavity tets and ring tets by 64-bit atomicMin of a
+//                 round-stamped priority key
+//   k_resolve     a candidate wins when it holds the minimum claim on all its
+//                 cavity tets
+//   k_shared      two winners whose cavities share a face both stay only if
+//                 that face remains Delaunay (exact insphere); else the worse
+//                 one steps back -- this exact test replaces a blanket
+//                 exclusion of neighbouring cavities
+//   k_alloc       recycled / fresh slots for the new tets
+//   k_write       new tets written, adjacency stitched by rotating around
+//                 boundary edges, cavity retired
+//   k_relocate    points whose tet was retired walk (exact orient3d) from a
+//                 tet of the inserting point; the rest keep their tet; the
+//                 uninserted list is compacted with warp-aggregated appends
+// Strata: points are Morton-sorted per cloud (counting sort) and inserted in
+// the reference's stratified stride order (src/gpu/mod.rs:533-600), each new
+// stratum located by a walk from its predecessor on the curve.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "engine.cuh"
+#include "exact.cuh"
+
+namespace wtet {
+
+constexpr uint32_t NONE = 0xFFFFFFFFu;
+constexpr uint32_t DEAD = 0xFFFFFFFFu;  // tv.x of a retired tet; tv.y then forwards to a live tet
+constexpr uint32_t INS_BIT = 0x80000000u;
+constexpr int SMALL_CAP = 80;           // cavity tets held per thread in the fast path
+constexpr uint32_t BIG_CAP = 1u << 16;  // cavity tets per large-cavity slot
+constexpr uint32_t BIG_SLOTS = 256;     // large cavities expanded per round
+constexpr uint32_t WALK_LIMIT = 1u << 22;
+constexpr int ROT_LIMIT = 1 << 16;
+constexpr int kMaxLevels = 15;
+
+enum : uint32_t {
+  kErrWalk = 1u << 0,
+  kErrCapacity = 1u << 1,
+  kErrRotate = 1u << 2,
+  kErrSeed = 1u << 3,
+  kErrPrec = ex::kErrPrecision,  // 1 << 4
+  kErrHull = 1u << 5,
+  kErrGuard = 1u << 6,  // an index failed a range guard (never expected)
+};
+
+struct Counters {
+  uint32_t n_next;        // uninserted points carried to the next round
+  uint32_t n_cand;        // candidates that completed a cavity
+  uint32_t pool_used;     // cavity-list pool entries
+  uint32_t alloc_used;    // tet slots handed out this round (virtual index)
+  uint32_t n_freed_next;  // tets retired this round
+  uint32_t big_used;      // large-cavity slots used
+  uint32_t n_inserted;    // winners this round
+  uint32_t err;           // error flags
+  unsigned long long walk_steps;
+  unsigned long long n_expanded;
+  unsigned long long n_big;
+  unsigned long long created;
+};
+
+// Everything a kernel needs, passed by value.
+struct Dev {
+  // vertices (internal ids)
+  float4* pts;
+  uint32_t* sos;     // SoS key = cloud-local input index (super vertices n_c..n_c+3)
+  uint32_t* vcloud;  // cloud of each vertex
+  uint32_t* vtet;    // a tet incident to each inserted vertex (hint, may be stale)
+  uint32_t* loc;     // containing tet of uninserted points; INS_BIT once inserted
+  uint8_t* bigflag;  // point needs the large-cavity path
+  // tets
+  uint4* tv;
+  uint4* tn;  // (tet << 2) | face, NONE on the super tetrahedron's hull
+  unsigned long long* ccav;
+  unsigned long long* cring;
+  uint4* nslot;
+  unsigned long long* vote;
+  uint32_t cap;
+  uint32_t nv;  // vertices (range guard)
+  // clouds
+  uint32_t* centry;  // a live tet of each cloud
+  // lists
+  uint32_t* active;
+  uint32_t* active_next;
+  uint32_t* cand;
+  uint32_t* cand_off;  // pool offset, or BIG flag | big slot
+  uint32_t* cand_len;
+  uint32_t* cand_base;
+  uint8_t* st1;  // candidate owns its whole cavity
+  uint8_t* st2;  // ... and no shared face with a better winner is violated
+  uint32_t* pool;
+  uint32_t pool_cap;
+  uint32_t* big;
+  uint32_t* freed_prev;
+  uint32_t* freed_next;
+  Counters* ctr;
+  int rule;
+};
+
+struct RoundArgs {
+  unsigned long long stamp;  // (~round) << 32
+  uint32_t round;
+  uint32_t n_active;
+  uint32_t n_freed_prev;
+  uint32_t tet_top;
+};
+
+__device__ __forceinline__ uint32_t comp(const uint4& v, int i) {
+  return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));
+}
+__device__ __forceinline__ void set_comp(uint4& v, int i, uint32_t x) {
+  if (i == 0) v.x = x;
+  else if (i == 1) v.y = x;
+  else if (i == 2) v.z = x;
+  else v.w = x;
+}
+__device__ __forceinline__ void load_pt(const float4* pts, uint32_t v, double* o) {
+  float4 q = pts[v];
+  o[0] = q.x;
+  o[1] = q.y;
+  o[2] = q.z;
+}
+
+// Bijective 32-bit mixer (murmur3 finaliser) -> distinct priorities per round.
+__device__ __forceinline__ uint32_t mix32(uint32_t h) {
+  h ^= h >> 16;
+  h *= 0x85ebca6bu;
+  h ^= h >> 13;
+  h *= 0xc2b2ae35u;
+  h ^= h >> 16;
+  return h;
+}
+__device__ __forceinline__ unsigned long long make_key(const RoundArgs& R, uint32_t p) {
+  return R.stamp | mix32(p ^ (R.round * 0x9E3779B9u));
+}
+
+// Appends `pred` lanes to a list through one atomic per warp.
+__device__ __forceinline__ uint32_t warp_append(uint32_t* ctr, bool pred) {
+  unsigned mask = __activemask();
+  unsigned ball = __ballot_sync(mask, pred);
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(mask) - 1;
+  uint32_t base = 0;
+  if (lane == leader && ball) base = atomicAdd(ctr, __popc(ball));
+  base = __shfl_sync(mask, base, leader);
+  return base + __popc(ball & ((1u << lane) - 1u));
+}
+
+__device__ __forceinline__ int o3d_sos(const double* a, const double* b, const double* c, const double* d,
+                                       uint32_t va, uint32_t vb, uint32_t vc, uint32_t vd, const uint32_t* sos,
+                                       uint32_t* err) {
+  int s = ex::orient3d(a, b, c, d, err);
+  if (s != 0) return s < 0 ? 1 : -1;
+  return ex::orient3d_sos_degenerate(a, b, c, d, sos[va], sos[vb], sos[vc], sos[vd]);
+}
+
+__device__ __forceinline__ int o4d_sos(const double* a, const double* b, const double* c, const double* d,
+                                       const double* e, uint32_t va, uint32_t vb, uint32_t vc, uint32_t vd,
+                                       uint32_t ve, const uint32_t* sos, uint32_t* err) {
+  int s = ex::insphere(a, b, c, d, e, err);
+  if (s != 0) return s;
+  return ex::orient4d_sos_degenerate(a, b, c, d, e, sos[va], sos[vb], sos[vc], sos[vd], sos[ve], err);
+}
+
+// Visibility walk with exact orient3d + SoS from tet t to the tet containing p.
+__device__ uint32_t walk_to(const Dev& D, uint32_t t, uint32_t p, const double* pp, uint32_t& steps) {
+  int entry = -1;
+  for (uint32_t s = 0; s < WALK_LIMIT; ++s) {
+    if (t >= D.cap) {
+      atomicOr(&D.ctr->err, kErrGuard);
+      return 0;
+    }
+    uint4 V = D.tv[t];
+    if (V.x >= D.nv || V.y >= D.nv || V.z >= D.nv || V.w >= D.nv) {
+      atomicOr(&D.ctr->err, kErrGuard);
+      return t;
+    }
+    uint32_t vv[4] = {V.x, V.y, V.z, V.w};
+    double P[4][3];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) load_pt(D.pts, vv[k], P[k]);
+    int moved = -1;
+    for (int i = 0; i < 4; ++i) {
+      int f = (i + int(s)) & 3;
+      if (f == entry) continue;
+      const double* q[4] = {P[0], P[1], P[2], P[3]};
+      uint32_t w[4] = {vv[0], vv[1], vv[2], vv[3]};
+      q[f] = pp;
+      w[f] = p;
+      if (o3d_sos(q[0], q[1], q[2], q[3], w[0], w[1], w[2], w[3], D.sos, &D.ctr->err) == -1) {
+        moved = f;
+        break;
+      }
+    }
+    if (moved < 0) {
+      steps += s + 1;
+      return t;
+    }
+    uint32_t n = comp(D.tn[t], moved);
+    if (n == NONE) {
+      atomicOr(&D.ctr->err, kErrWalk);
+      return t;
+    }
+    t = n >> 2;
+    entry = int(n & 3);
+  }
+  atomicOr(&D.ctr->err, kErrWalk);
+  return t;
+}
+
+// ---------------------------------------------------------------- setup ----
+
+// Ordered-uint encoding of floats for atomic min / max.
+__device__ __forceinline__ uint32_t f2o(float f) {
+  uint32_t b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float o2f(uint32_t o) {
+  return __uint_as_float((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
+}
+
+__device__ __forceinline__ uint32_t cloud_of(const uint64_t* off, uint32_t nc, uint64_t i) {
+  uint32_t lo = 0, hi = nc;  // off[lo] <= i < off[hi]
+  while (hi - lo > 1) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (off[mid] <= i) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Per-cloud bounding box (src/lib.rs:315-323): block-reduce, then atomics.
+__global__ void k_bbox(const float* xyz, const uint64_t* off, uint32_t nc, uint64_t n, uint32_t* mn, uint32_t* mx) {
+  __shared__ uint32_t smn[3], smx[3];
+  __shared__ uint32_t scloud_first, scloud_last;
+  uint64_t base = uint64_t(blockIdx.x) * blockDim.x;
+  uint64_t i = base + threadIdx.x;
+  if (threadIdx.x == 0) {
+    smn[0] = smn[1] = smn[2] = 0xFFFFFFFFu;
+    smx[0] = smx[1] = smx[2] = 0u;
+    scloud_first = cloud_of(off, nc, base);
+    uint64_t last = min(base + blockDim.x, n) - 1;
+    scloud_last = cloud_of(off, nc, last);
+  }
+  __syncthreads();
+  bool uniform = scloud_first == scloud_last;
+  if (i < n) {
+    uint32_t c = uniform ? scloud_first : cloud_of(off, nc, i);
+    for (int k = 0; k < 3; ++k) {
+      float v = xyz[3 * i + k];
+      if (v != v) continue;  // NaN is ignored, as f32::min / f32::max do
+      uint32_t o = f2o(v);
+      if (uniform) {
+        atomicMin(&smn[k], o);
+        atomicMax(&smx[k], o);
+      } else {
+        atomicMin(&mn[3 * c + k], o);
+        atomicMax(&mx[3 * c + k], o);
+      }
+    }
+  }
+  __syncthreads();
+  if (uniform && threadIdx.x < 3) {
+    atomicMin(&mn[3 * scloud_first + threadIdx.x], smn[threadIdx.x]);
+    atomicMax(&mx[3 * scloud_first + threadIdx.x], smx[threadIdx.x]);
+  }
+}
+
+struct CloudInfo {
+  uint64_t off;      // first input point
+  uint32_t n;        // points
+  uint32_t vbase;    // internal id of its first point (super vertices follow the points)
+  uint32_t bbase;    // first Morton bucket
+  uint32_t bbits;    // bits per axis of its buckets
+  uint32_t top;      // top stratum level (log2 of the initial stride)
+  uint32_t pad;
+};
+
+__device__ __forceinline__ uint32_t expand10(uint32_t v) {
+  v = (v | (v << 16)) & 0x030000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+// Normalises (src/lib.rs:325-334, f32 arithmetic) and buckets each point by a
+// per-cloud Morton code; counts bucket sizes.
+__global__ void k_normalize(const float* xyz, const uint64_t* off, const CloudInfo* ci, uint32_t nc, uint64_t n,
+                            const uint32_t* mn, const uint32_t* mx, float4* tmp, uint32_t* bucket,
+                            uint32_t* hist) {
+  uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t c = cloud_of(off, nc, i);
+  float lo[3], ext[3];
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = o2f(mn[3 * c + k]);
+    ext[k] = o2f(mx[3 * c + k]) - lo[k];
+  }
+  float s = fmaxf(fmaxf(fmaxf(ext[0], ext[1]), ext[2]), 1e-10f);
+  float q[3];
+  for (int k = 0; k < 3; ++k) q[k] = __fdiv_rn(__fsub_rn(xyz[3 * i + k], lo[k]), s);
+  tmp[i] = make_float4(q[0], q[1], q[2], 0.f);
+  CloudInfo C = ci[c];
+  uint32_t res = 1u << C.bbits;
+  uint32_t code[3];
+  for (int k = 0; k < 3; ++k) {
+    float v = q[k] * float(res);
+    uint32_t u = (v > 0.f) ? (v >= float(res) ? res - 1 : uint32_t(v)) : 0u;
+    code[k] = u;
+  }
+  uint32_t b = C.bbase + ((expand10(code[2]) << 2) | (expand10(code[1]) << 1) | expand10(code[0]));
+  bucket[i] = b;
+  atomicAdd(&hist[b], 1u);
+}
+
+// Scatters points into Morton order inside their cloud.
+__global__ void k_scatter_points(const uint64_t* off, const CloudInfo* ci, uint32_t nc, uint64_t n,
+                                 const float4* tmp, const uint32_t* bucket, uint32_t* cursor, Dev D) {
+  uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t c = cloud_of(off, nc, i);
+  uint32_t pos = atomicAdd(&cursor[bucket[i]], 1u);  // global Morton position
+  uint32_t v = pos + 4u * c;                          // skip the super vertices of earlier clouds
+  D.pts[v] = tmp[i];
+  D.sos[v] = uint32_t(i - ci[c].off);
+  D.vcloud[v] = c;
+  D.loc[v] = 0;
+  D.bigflag[v] = 0;
+  D.vtet[v] = NONE;
+}
+
+// Super vertices (src/gpu/mod.rs:151-158) and the initial super tet of every
+// cloud, oriented with orient3d_sos > 0 (src/phase2.rs:404-410).
+__global__ void k_init_clouds(const CloudInfo* ci, uint32_t nc, Dev D) {
+  uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  CloudInfo C = ci[c];
+  const float S[4][3] = {{-100.f, -100.f, -100.f}, {400.f, -100.f, -100.f}, {-100.f, 400.f, -100.f},
+                         {-100.f, -100.f, 400.f}};
+  uint32_t s0 = C.vbase + C.n;
+  for (int k = 0; k < 4; ++k) {
+    D.pts[s0 + k] = make_float4(S[k][0], S[k][1], S[k][2], 0.f);
+    D.sos[s0 + k] = C.n + k;
+    D.vcloud[s0 + k] = c;
+    D.vtet[s0 + k] = c;
+    D.loc[s0 + k] = INS_BIT;
+  }
+  double P[4][3];
+  for (int k = 0; k < 4; ++k) load_pt(D.pts, s0 + k, P[k]);
+  int o = o3d_sos(P[0], P[1], P[2], P[3], s0, s0 + 1, s0 + 2, s0 + 3, D.sos, &D.ctr->err);
+  D.tv[c] = (o > 0) ? make_uint4(s0, s0 + 1, s0 + 2, s0 + 3) : make_uint4(s0 + 1, s0, s0 + 2, s0 + 3);
+  D.tn[c] = make_uint4(NONE, NONE, NONE, NONE);
+  D.centry[c] = c;
+}
+
+// ---------------------------------------------------------------- rounds ----
+
+// Locates the points of one stratum: walk from the tet of the point one
+// stride earlier on the Morton curve (a point of an earlier stratum: its tet
+// once inserted, else the tet that still contains it).  The located points are
+// appended to the uninserted list at position `base`.
+__global__ void k_activate(Dev D, const CloudInfo* ci, const uint64_t* lvl_off, uint32_t nc, uint32_t level,
+                           uint32_t total, uint32_t base) {
+  uint32_t steps = 0;
+  for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = nc;
+    while (hi - lo > 1) {
+      uint32_t mid = (lo + hi) >> 1;
+      if (lvl_off[mid] <= idx) lo = mid;
+      else hi = mid;
+    }
+    uint32_t c = lo;
+    CloudInfo C = ci[c];
+    uint32_t k = idx - uint32_t(lvl_off[c]);
+    uint32_t stride = 1u << level;
+    uint32_t pos = (level == C.top) ? k * stride : (2u * k + 1u) * stride;
+    uint32_t p = C.vbase + pos;
+    uint32_t t = NONE;
+    if (level < C.top) {
+      uint32_t hv = p - stride;
+      uint32_t hl = D.loc[hv];
+      uint32_t h = (hl & INS_BIT) ? D.vtet[hv] : hl;
+      if (h != NONE && h < D.cap) {
+        uint4 V = D.tv[h];
+        if (V.x < D.nv && D.vcloud[V.x] == c) t = h;
+      }
+    }
+    if (t == NONE) t = D.centry[c];
+    double pp[3];
+    load_pt(D.pts, p, pp);
+    D.loc[p] = walk_to(D, t, p, pp, steps);
+    D.bigflag[p] = 0;
+    D.active[base + idx] = p;
+  }
+  if (steps) atomicAdd(&D.ctr->walk_steps, (unsigned long long)steps);
+}
+
+// Vote score: larger = inserted first.  Circumcenter rule: depth of p inside
+// the circumsphere (f32 insphere, src/shaders/vote.wgsl:401-494 semantics);
+// centroid rule: inverse squared distance to the centroid.
+__device__ __forceinline__ float vote_score(const float4* pts, uint4 V, float4 q, int rule) {
+  float4 a = pts[V.x], b = pts[V.y], c = pts[V.z], d = pts[V.w];
+  if (rule == 1) {
+    float cx = 0.25f * (a.x + b.x + c.x + d.x) - q.x;
+    float cy = 0.25f * (a.y + b.y + c.y + d.y) - q.y;
+    float cz = 0.25f * (a.z + b.z + c.z + d.z) - q.z;
+    return 1.0f / (1e-30f + cx * cx + cy * cy + cz * cz);
+  }
+  float aex = a.x - q.x, aey = a.y - q.y, aez = a.z - q.z;
+  float bex = b.x - q.x, bey = b.y - q.y, bez = b.z - q.z;
+  float cex = c.x - q.x, cey = c.y - q.y, cez = c.z - q.z;
+  float dex = d.x - q.x, dey = d.y - q.y, dez = d.z - q.z;
+  float ab = aex * bey - bex * aey, bc = bex * cey - cex * bey, cd = cex * dey - dex * cey;
+  float da = dex * aey - aex * dey, ac = aex * cey - cex * aey, bd = bex * dey - dex * bey;
+  float abc = aez * bc - bez * ac + cez * ab, bcd = bez * cd - cez * bd + dez * bc;
+  float cda = cez * da + dez * ac + aez * cd, dab = dez * ab + aez * bd + bez * da;
+  float al = aex * aex + aey * aey + aez * aez, bl = bex * bex + bey * bey + bez * bez;
+  float cl = cex * cex + cey * cey + cez * cez, dl = dex * dex + dey * dey + dez * dez;
+  float det = (dl * abc - cl * dab) + (bl * cda - al * bcd);
+  float depth = -det;  // tets have Shewchuk orient3d < 0, so inside means det < 0
+  return (depth > 0.f && depth < 3.0e38f) ? depth : 0.f;
+}
+
+__global__ void k_vote(Dev D, RoundArgs R) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < R.n_active; i += gridDim.x * blockDim.x) {
+    uint32_t p = D.active[i];
+    uint32_t t = D.loc[p];
+    if (t >= D.cap) {
+      atomicOr(&D.ctr->err, kErrGuard);
+      continue;
+    }
+    uint4 V = D.tv[t];
+    if (V.x >= D.nv || V.y >= D.nv || V.z >= D.nv || V.w >= D.nv) {
+      atomicOr(&D.ctr->err, kErrGuard);
+      continue;
+    }
+    float sc = vote_score(D.pts, V, D.pts[p], D.rule);
+    unsigned long long key = ((unsigned long long)__float_as_uint(sc) << 32) | (unsigned long long)(~p);
+    atomicMax(&D.vote[t], key);
+  }
+}
+
+// Inverse of mix32: recovers the point that owns a claim key.
+__device__ __forceinline__ uint32_t unmix32(uint32_t h) {
+  h ^= h >> 16;
+  h *= 0x7ed1b41du;
+  h ^= (h >> 13) ^ (h >> 26);
+  h *= 0xa5cb9243u;
+  h ^= h >> 16;
+  return h;
+}
+__device__ __forceinline__ uint32_t key_owner(const RoundArgs& R, unsigned long long key) {
+  return unmix32(uint32_t(key)) ^ (R.round * 0x9E3779B9u);
+}
+__device__ __forceinline__ bool this_round(const RoundArgs& R, unsigned long long key) {
+  return (key >> 32) == (R.stamp >> 32);
+}
+
+// Grows the cavity of p (tets whose circumsphere holds p, src/phase2.rs:428-470)
+// from its containing tet t0, claiming each cavity tet by atomicMin of the
+// round's key.  Returns K > 0, 0 when a better candidate owns part of the
+// cavity, -1 when the cavity exceeds cap.
+__device__ int grow_cavity(const Dev& D, uint32_t p, const double* pp, uint32_t t0, unsigned long long key,
+                           uint32_t* cav, uint32_t cap) {
+  unsigned long long old = atomicMin(&D.ccav[t0], key);
+  if (old < key) return 0;
+  cav[0] = t0;
+  uint32_t K = 1;
+  for (uint32_t i = 0; i < K; ++i) {
+    uint32_t c = cav[i];
+    uint4 N = D.tn[c];
+    for (int f = 0; f < 4; ++f) {
+      uint32_t nb = comp(N, f);
+      if (nb == NONE) continue;
+      uint32_t nt = nb >> 2;
+      if (nt >= D.cap) {
+        atomicOr(&D.ctr->err, kErrGuard);
+        return 0;
+      }
+      if (__ldcg(&D.ccav[nt]) == key) continue;
+      if (__ldcg(&D.cring[nt]) == key) continue;  // already found outside
+      uint4 W = D.tv[nt];
+      if (W.x >= D.nv || W.y >= D.nv || W.z >= D.nv || W.w >= D.nv) {
+        atomicOr(&D.ctr->err, kErrGuard);
+        return 0;
+      }
+      double P[4][3];
+      load_pt(D.pts, W.x, P[0]);
+      load_pt(D.pts, W.y, P[1]);
+      load_pt(D.pts, W.z, P[2]);
+      load_pt(D.pts, W.w, P[3]);
+      int s = o4d_sos(P[0], P[1], P[2], P[3], pp, W.x, W.y, W.z, W.w, p, D.sos, &D.ctr->err);
+      if (s < 0) {
+        old = atomicMin(&D.ccav[nt], key);
+        if (old < key) return 0;
+        if (old == key) continue;
+        if (K >= cap) return -1;
+        cav[K++] = nt;
+      } else {
+        D.cring[nt] = key;  // memo for this candidate only
+      }
+    }
+  }
+  return int(K);
+}
+
+__global__ void __launch_bounds__(256) k_expand(Dev D, RoundArgs R) {
+  uint32_t cav[SMALL_CAP];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < R.n_active; i += gridDim.x * blockDim.x) {
+    uint32_t p = D.active[i];
+    uint32_t t = D.loc[p];
+    if (D.bigflag[p] || t >= D.cap) continue;
+    if (uint32_t(D.vote[t]) != ~p) continue;
+    D.st1[p] = 0;
+    D.st2[p] = 0;
+    unsigned long long key = make_key(R, p);
+    double pp[3];
+    load_pt(D.pts, p, pp);
+    int K = grow_cavity(D, p, pp, t, key, cav, SMALL_CAP);
+    atomicAdd(&D.ctr->n_expanded, 1ull);
+    if (K < 0) {
+      // Its partial claims carry this round's key, so the large path takes it
+      // from the next round on (k_relocate promotes 2 -> 1).
+      D.bigflag[p] = 2;
+      continue;
+    }
+    if (K == 0) continue;
+    uint32_t off = atomicAdd(&D.ctr->pool_used, uint32_t(K));
+    if (off + uint32_t(K) > D.pool_cap) continue;  // pool full: retry next round
+    for (int k = 0; k < K; ++k) D.pool[off + k] = cav[k];
+    uint32_t ci = atomicAdd(&D.ctr->n_cand, 1u);
+    D.cand[ci] = p;
+    D.cand_off[ci] = off;
+    D.cand_len[ci] = uint32_t(K);
+  }
+}
+
+// Large cavities: one thread per point, cavity list in a global slot.
+__global__ void k_expand_big(Dev D, RoundArgs R) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < R.n_active; i += gridDim.x * blockDim.x) {
+    uint32_t p = D.active[i];
+    if (D.bigflag[p] != 1) continue;
+    uint32_t t = D.loc[p];
+    if (t >= D.cap) continue;
+    if (uint32_t(D.vote[t]) != ~p) continue;
+    uint32_t slot = atomicAdd(&D.ctr->big_used, 1u);
+    if (slot >= BIG_SLOTS) continue;
+    D.st1[p] = 0;
+    D.st2[p] = 0;
+    uint32_t* cav = D.big + size_t(slot) * BIG_CAP;
+    unsigned long long key = make_key(R, p);
+    double pp[3];
+    load_pt(D.pts, p, pp);
+    int K = grow_cavity(D, p, pp, t, key, cav, BIG_CAP);
+    atomicAdd(&D.ctr->n_big, 1ull);
+    if (K <= 0) continue;
+    uint32_t ci = atomicAdd(&D.ctr->n_cand, 1u);
+    D.cand[ci] = p;
+    D.cand_off[ci] = 0x80000000u | slot;
+    D.cand_len[ci] = uint32_t(K);
+  }
+}
+
+__device__ __forceinline__ const uint32_t* cand_cavity(const Dev& D, uint32_t off) {
+  return (off & 0x80000000u) ? D.big + size_t(off & 0x7FFFFFFFu) * BIG_CAP : D.pool + off;
+}
+
+// A candidate wins its cavity when it holds the minimum claim on every tet.
+__global__ void k_resolve(Dev D, RoundArgs R) {
+  const uint32_t ncand = *(volatile uint32_t*)&D.ctr->n_cand;
+  for (uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x; ci < ncand; ci += gridDim.x * blockDim.x) {
+    uint32_t p = D.cand[ci];
+    uint32_t K = D.cand_len[ci];
+    const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
+    unsigned long long key = make_key(R, p);
+    bool win = true;
+    for (uint32_t i = 0; i < K; ++i)
+      if (__ldcg(&D.ccav[cav[i]]) != key) {
+        win = false;
+        break;
+      }
+    D.st1[p] = win ? 1 : 0;
+  }
+}
+
+// Two winners whose cavities share a face f may both insert iff f stays
+// Delaunay: the better winner q must lie outside the circumsphere of the
+// worse winner p's new tet on f (then either insertion order gives the same
+// tets).  The worse one of a violating pair steps back.
+__global__ void k_shared(Dev D, RoundArgs R) {
+  const uint32_t ncand = *(volatile uint32_t*)&D.ctr->n_cand;
+  for (uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x; ci < ncand; ci += gridDim.x * blockDim.x) {
+    uint32_t p = D.cand[ci];
+    if (!D.st1[p]) {
+      D.st2[p] = 0;
+      continue;
+    }
+    uint32_t K = D.cand_len[ci];
+    const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
+    unsigned long long key = make_key(R, p);
+    bool ok = true;
+    double pp[3];
+    load_pt(D.pts, p, pp);
+    for (uint32_t i = 0; i < K && ok; ++i) {
+      uint32_t c = cav[i];
+      uint4 N = D.tn[c];
+      for (int f = 0; f < 4; ++f) {
+        uint32_t nb = comp(N, f);
+        if (nb == NONE) continue;
+        unsigned long long cc = __ldcg(&D.ccav[nb >> 2]);
+        if (cc >= key || !this_round(R, cc)) continue;
+        uint32_t q = key_owner(R, cc);
+        if (q >= D.nv || !D.st1[q]) continue;
+        uint4 V = D.tv[c];
+        uint32_t w[4] = {V.x, V.y, V.z, V.w};
+        double P[4][3];
+        for (int k = 0; k < 4; ++k) load_pt(D.pts, w[k], P[k]);
+        P[f][0] = pp[0];
+        P[f][1] = pp[1];
+        P[f][2] = pp[2];
+        w[f] = p;
+        double qq[3];
+        load_pt(D.pts, q, qq);
+        if (o4d_sos(P[0], P[1], P[2], P[3], qq, w[0], w[1], w[2], w[3], q, D.sos, &D.ctr->err) < 0) {
+          ok = false;
+          break;
+        }
+      }
+    }
+    D.st2[p] = ok ? 1 : 0;
+  }
+}
+
+__device__ __forceinline__ uint32_t slot_of(const Dev& D, const RoundArgs& R, uint32_t v) {
+  return v < R.n_freed_prev ? D.freed_prev[v] : R.tet_top + (v - R.n_freed_prev);
+}
+
+__device__ __forceinline__ bool boundary_face(const Dev& D, uint32_t nb, unsigned long long key) {
+  return nb == NONE || __ldcg(&D.ccav[nb >> 2]) != key;
+}
+
+// Hands out one slot per boundary face (recycled slots first, then fresh ones).
+__global__ void k_alloc(Dev D, RoundArgs R) {
+  const uint32_t ncand = *(volatile uint32_t*)&D.ctr->n_cand;
+  for (uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x; ci < ncand; ci += gridDim.x * blockDim.x) {
+    uint32_t p = D.cand[ci];
+    if (!D.st2[p]) continue;
+    uint32_t K = D.cand_len[ci];
+    const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
+    unsigned long long key = make_key(R, p);
+    uint32_t F = 0;
+    for (uint32_t i = 0; i < K; ++i) {
+      uint4 N = D.tn[cav[i]];
+      for (int f = 0; f < 4; ++f) F += boundary_face(D, comp(N, f), key);
+    }
+    uint32_t base = atomicAdd(&D.ctr->alloc_used, F);
+    uint32_t last = base + F;
+    if (last > R.n_freed_prev && R.tet_top + (last - R.n_freed_prev) > D.cap) {
+      atomicOr(&D.ctr->err, kErrCapacity);
+      D.st2[p] = 0;
+      continue;
+    }
+    uint32_t j = 0;
+    for (uint32_t i = 0; i < K; ++i) {
+      uint32_t c = cav[i];
+      uint4 N = D.tn[c];
+      uint4 S = make_uint4(NONE, NONE, NONE, NONE);
+      for (int f = 0; f < 4; ++f)
+        if (boundary_face(D, comp(N, f), key)) set_comp(S, f, slot_of(D, R, base + j++));
+      D.nslot[c] = S;
+    }
+    D.cand_base[ci] = base;
+  }
+}
+
+// Writes the new tets of every winner.  Faces through p are matched by
+// rotating around the boundary edge inside the cavity; a boundary face shared
+// with another winner's cavity links to that winner's new tet.
+__global__ void __launch_bounds__(128) k_write(Dev D, RoundArgs R) {
+  const uint32_t ncand = *(volatile uint32_t*)&D.ctr->n_cand;
+  for (uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x; ci < ncand; ci += gridDim.x * blockDim.x) {
+    uint32_t p = D.cand[ci];
+    if (!D.st2[p]) continue;
+    uint32_t K = D.cand_len[ci];
+    const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
+    unsigned long long key = make_key(R, p);
+    uint32_t F = 0;
+    bool bad = false;
+    for (uint32_t i = 0; i < K; ++i) {
+      uint32_t c = cav[i];
+      uint4 V = D.tv[c];
+      uint4 N = D.tn[c];
+      uint4 S = D.nslot[c];
+      for (int f = 0; f < 4; ++f) {
+        uint32_t s = comp(S, f);
+        if (s == NONE) continue;
+        ++F;
+        uint32_t outer = comp(N, f);
+        bool shared = false;
+        uint32_t link_out = outer;
+        if (outer != NONE) {
+          uint32_t o = outer >> 2;
+          unsigned long long cc = __ldcg(&D.ccav[o]);
+          if (cc != key && this_round(R, cc)) {
+            uint32_t q = key_owner(R, cc);
+            if (q < D.nv && D.st2[q]) {
+              shared = true;
+              link_out = (comp(D.nslot[o], outer & 3) << 2) | (outer & 3);
+            }
+          }
+        }
+        uint4 nv = V;
+        set_comp(nv, f, p);
+        uint4 nn = make_uint4(NONE, NONE, NONE, NONE);
+        set_comp(nn, f, link_out);
+        for (int k = 0; k < 4; ++k) {
+          if (k == f) continue;
+          uint32_t cur = c;
+          uint4 Vc = V;
+          int kc = k, ms = f;
+          uint32_t link = NONE;
+          for (int it = 0; it < ROT_LIMIT; ++it) {
+            uint32_t nb = comp(D.tn[cur], kc);
+            if (boundary_face(D, nb, key)) {
+              link = (comp(D.nslot[cur], kc) << 2) | uint32_t(ms);
+              break;
+            }
+            uint32_t nt = nb >> 2;
+            if (nt >= D.cap) break;
+            int entry = int(nb & 3);
+            uint32_t x = comp(Vc, ms);
+            uint4 W = D.tv[nt];
+            int kx = -1;
+            for (int q = 0; q < 4; ++q)
+              if (comp(W, q) == x) kx = q;
+            if (kx < 0) break;
+            cur = nt;
+            Vc = W;
+            kc = kx;
+            ms = entry;
+          }
+          if (link == NONE) bad = true;
+          set_comp(nn, k, link);
+        }
+        D.tv[s] = nv;
+        D.tn[s] = nn;
+        if (outer != NONE && !shared && (outer >> 2) < D.cap) {
+          uint32_t* w = reinterpret_cast<uint32_t*>(&D.tn[outer >> 2]) + (outer & 3);
+          *w = (s << 2) | uint32_t(f);
+        }
+      }
+    }
+    if (bad) atomicOr(&D.ctr->err, kErrRotate);
+    // Retire the cavity, forwarding to a new tet of p.
+    uint32_t s0 = slot_of(D, R, D.cand_base[ci]);
+    for (uint32_t i = 0; i < K; ++i) {
+      uint32_t c = cav[i];
+      D.tv[c] = make_uint4(DEAD, s0, 0u, 0u);
+    }
+    uint32_t fbase = atomicAdd(&D.ctr->n_freed_next, K);
+    for (uint32_t i = 0; i < K; ++i) D.freed_next[fbase + i] = cav[i];
+    D.vtet[p] = s0;
+    D.loc[p] |= INS_BIT;
+    D.centry[D.vcloud[p]] = s0;
+    D.bigflag[p] = 0;
+    atomicAdd(&D.ctr->n_inserted, 1u);
+    atomicAdd(&D.ctr->created, (unsigned long long)F);
+  }
+}
+
+// Clears the votes, relocates points whose tet was retired, and compacts the
+// uninserted list.
+__global__ void k_relocate(Dev D, RoundArgs R) {
+  uint32_t steps = 0;
+  for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < R.n_active; i0 += gridDim.x * blockDim.x) {
+    uint32_t i = i0 + threadIdx.x;
+    bool keep = false;
+    uint32_t p = 0;
+    if (i < R.n_active) {
+      p = D.active[i];
+      uint32_t L = D.loc[p];
+      uint32_t t = L & ~INS_BIT;
+      if (t >= D.cap) {
+        atomicOr(&D.ctr->err, kErrGuard);
+        t = 0;
+        L |= INS_BIT;
+      }
+      D.vote[t] = 0ull;
+      if (!(L & INS_BIT)) {
+        keep = true;
+        if (D.bigflag[p] == 2) D.bigflag[p] = 1;
+        uint4 V = D.tv[t];
+        if (V.x == DEAD) {
+          double pp[3];
+          load_pt(D.pts, p, pp);
+          D.loc[p] = walk_to(D, V.y, p, pp, steps);
+        }
+      }
+    }
+    uint32_t slot = warp_append(&D.ctr->n_next, keep);
+    if (keep) D.active_next[slot] = p;
+  }
+  if (steps) atomicAdd(&D.ctr->walk_steps, (unsigned long long)steps);
+}
+
+// --------------------------------------------------------------- output ----
+
+// Counts live tets per cloud and records the hull faces (no neighbour).
+__global__ void k_count(Dev D, uint32_t tet_top, uint32_t* ccount, uint32_t* hullcnt, uint2* hull) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < tet_top; t += gridDim.x * blockDim.x) {
+    uint4 V = D.tv[t];
+    if (V.x == DEAD) continue;
+    uint32_t c = D.vcloud[V.x];
+    atomicAdd(&ccount[c], 1u);
+    uint4 N = D.tn[t];
+    for (int f = 0; f < 4; ++f) {
+      if (comp(N, f) == NONE) {
+        uint32_t h = atomicAdd(&hullcnt[c], 1u);
+        if (h < 4) hull[4 * c + h] = make_uint2(t, uint32_t(f));
+        else atomicOr(&D.ctr->err, kErrHull);
+      }
+    }
+  }
+}
+
+__global__ void k_number(Dev D, uint32_t tet_top, uint32_t* cfill, uint32_t* newid) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < tet_top; t += gridDim.x * blockDim.x) {
+    uint4 V = D.tv[t];
+    if (V.x == DEAD) continue;
+    uint32_t c = D.vcloud[V.x];
+    newid[t] = atomicAdd(&cfill[c], 1u);
+  }
+}
+
+__global__ void k_emit(Dev D, uint32_t tet_top, const uint32_t* newid, const uint64_t* coff, uint32_t* out_t,
+                       uint32_t* out_a) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < tet_top; t += gridDim.x * blockDim.x) {
+    uint4 V = D.tv[t];
+    if (V.x == DEAD) continue;
+    uint32_t c = D.vcloud[V.x];
+    uint64_t row = coff[c] + newid[t];
+    uint4 N = D.tn[t];
+    uint4 ov = make_uint4(D.sos[V.x], D.sos[V.y], D.sos[V.z], D.sos[V.w]);
+    uint4 oa;
+    for (int f = 0; f < 4; ++f) {
+      uint32_t nb = comp(N, f);
+      if (nb != NONE && (nb >> 2) >= tet_top) {
+        atomicOr(&D.ctr->err, kErrGuard);
+        nb = NONE;
+      }
+      set_comp(oa, f, nb == NONE ? NONE : ((newid[nb >> 2] << 5) | (nb & 3)));
+    }
+    reinterpret_cast<uint4*>(out_t)[row] = ov;
+    reinterpret_cast<uint4*>(out_a)[row] = oa;
+  }
+}
+
+// Four infinity tets per cloud on the super tetrahedron's hull faces.
+__global__ void k_infinity(Dev D, const CloudInfo* ci, uint32_t nc, const uint32_t* ccount,
+                           const uint32_t* hullcnt, const uint2* hull, const uint32_t* newid, const uint64_t* coff,
+                           uint32_t* out_t, uint32_t* out_a) {
+  uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  if (hullcnt[c] != 4) {
+    atomicOr(&D.ctr->err, kErrHull);
+    return;
+  }
+  const uint32_t inf = ci[c].n + 4;
+  uint32_t fv[4][3];  // the non-infinity vertices of each infinity tet (output ids)
+  uint4 rows[4];
+  uint32_t base = ccount[c];
+  for (int j = 0; j < 4; ++j) {
+    uint2 h = hull[4 * c + j];
+    uint4 V = D.tv[h.x];
+    uint32_t w[4] = {D.sos[V.x], D.sos[V.y], D.sos[V.z], D.sos[V.w]};
+    w[h.y] = inf;
+    int a = -1, b = -1;
+    for (int q = 0; q < 4; ++q)
+      if (q != int(h.y)) {
+        if (a < 0) a = q;
+        else if (b < 0) b = q;
+      }
+    uint32_t tmp = w[a];
+    w[a] = w[b];
+    w[b] = tmp;
+    rows[j] = make_uint4(w[0], w[1], w[2], w[3]);
+    int k = 0;
+    for (int q = 0; q < 4; ++q)
+      if (q != int(h.y)) fv[j][k++] = w[q];
+  }
+  for (int j = 0; j < 4; ++j) {
+    uint2 h = hull[4 * c + j];
+    uint64_t row = coff[c] + base + j;
+    uint32_t w[4] = {rows[j].x, rows[j].y, rows[j].z, rows[j].w};
+    uint32_t adj[4];
+    for (int q = 0; q < 4; ++q) {
+      if (q == int(h.y)) {
+        adj[q] = (newid[h.x] << 5) | h.y;
+        continue;
+      }
+      // Face opposite slot q holds inf and the two other face vertices.
+      uint32_t e[2];
+      int ne = 0;
+      for (int r = 0; r < 4; ++r)
+        if (r != q && r != int(h.y)) e[ne++] = w[r];
+      adj[q] = NONE;
+      for (int o = 0; o < 4; ++o) {
+        if (o == j) continue;
+        bool ha = false, hb = false;
+        for (int r = 0; r < 3; ++r) {
+          ha |= fv[o][r] == e[0];
+          hb |= fv[o][r] == e[1];
+        }
+        if (ha && hb) {
+          uint32_t ow[4] = {rows[o].x, rows[o].y, rows[o].z, rows[o].w};
+          int os = -1;
+          for (int r = 0; r < 4; ++r)
+            if (ow[r] != inf && ow[r] != e[0] && ow[r] != e[1]) os = r;
+          adj[q] = ((base + o) << 5) | uint32_t(os);
+        }
+      }
+    }
+    reinterpret_cast<uint4*>(out_t)[row] = rows[j];
+    reinterpret_cast<uint4*>(out_a)[row] = make_uint4(adj[0], adj[1], adj[2], adj[3]);
+    // The regular tet's hull face points at this infinity tet.
+    uint64_t rrow = coff[c] + newid[h.x];
+    out_a[4 * rrow + h.y] = ((base + j) << 5) | h.y;
+  }
+}
+
+// ----------------------------------------------------------- scan utils ----
+
+__global__ void k_scan_blocks(const uint32_t* in, uint32_t* out, uint32_t* sums, uint32_t n) {
+  __shared__ uint32_t warp_tot[32];
+  const uint32_t per = 4;
+  uint32_t base = blockIdx.x * blockDim.x * per;
+  uint32_t v[per];
+  uint32_t local = 0;
+  for (uint32_t k = 0; k < per; ++k) {
+    uint32_t i = base + threadIdx.x * per + k;
+    v[k] = i < n ? in[i] : 0u;
+    local += v[k];
+  }
+  uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = local;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+    if (lane >= uint32_t(o)) x += y;
+  }
+  if (lane == 31) warp_tot[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < (blockDim.x >> 5) ? warp_tot[lane] : 0u;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+      if (lane >= uint32_t(o)) w += y;
+    }
+    warp_tot[lane] = w;
+  }
+  __syncthreads();
+  uint32_t excl = x - local + (warp ? warp_tot[warp - 1] : 0u);
+  for (uint32_t k = 0; k < per; ++k) {
+    uint32_t i = base + threadIdx.x * per + k;
+    if (i < n) out[i] = excl;
+    excl += v[k];
+  }
+  if (threadIdx.x == blockDim.x - 1) sums[blockIdx.x] = excl;
+}
+
+__global__ void k_scan_add(uint32_t* out, const uint32_t* sums, uint32_t n) {
+  uint32_t base = blockIdx.x * blockDim.x * 4;
+  uint32_t add = sums[blockIdx.x];
+  for (uint32_t k = 0; k < 4; ++k) {
+    uint32_t i = base + threadIdx.x * 4 + k;
+    if (i < n) out[i] += add;
+  }
+}
+
+// ------------------------------------------------------------- host side ----
+
+namespace {
+
+void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw Error{WTET_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
+}
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void reserve(size_t want, const char* what) {
+    if (want <= n) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    ck(cudaMalloc(&p, std::max<size_t>(want, 1) * sizeof(T)), what);
+    n = want;
+  }
+  void grow_keep(size_t want, size_t used, cudaStream_t s, const char* what) {
+    if (want <= n) return;
+    T* q = nullptr;
+    ck(cudaMalloc(&q, want * sizeof(T)), what);
+    if (p && used) ck(cudaMemcpyAsync(q, p, used * sizeof(T), cudaMemcpyDeviceToDevice, s), what);
+    ck(cudaStreamSynchronize(s), what);
+    if (p) cudaFree(p);
+    p = q;
+    n = want;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+// Exclusive scan in place over n u32 (recursive over block sums).
+void scan_u32(uint32_t* d, uint32_t n, cudaStream_t s, std::vector<DBuf<uint32_t>>& tmp, int depth = 0) {
+  if (n == 0) return;
+  const uint32_t threads = 256, per_block = threads * 4;
+  uint32_t blocks = (n + per_block - 1) / per_block;
+  if (int(tmp.size()) <= depth) tmp.resize(depth + 1);
+  tmp[depth].reserve(size_t(blocks) + 1, "scan sums");
+  k_scan_blocks<<<blocks, threads, 0, s>>>(d, d, tmp[depth].p, n);
+  if (blocks > 1) {
+    scan_u32(tmp[depth].p, blocks, s, tmp, depth + 1);
+    k_scan_add<<<blocks, threads, 0, s>>>(d, tmp[depth].p, n);
+  }
+}
+
+uint32_t initial_stride_log2(uint64_t n) {
+  // src/gpu/mod.rs:533-548
+  double sq = std::sqrt(double(n));
+  double scaled = n > 100000 ? sq * 2.0 : sq;
+  double stride = std::min(std::max(scaled, 64.0), 16384.0);
+  return uint32_t(std::ceil(std::log2(stride)));
+}
+
+uint64_t level_count(uint64_t n, uint32_t level, uint32_t top) {
+  if (level > top) return 0;
+  uint64_t s = 1ull << level;
+  if (level == top) return (n + s - 1) / s;
+  if (n <= s) return 0;
+  return (n - s - 1) / (2 * s) + 1;
+}
+
+}  // namespace
+
+struct Workspace {
+  DBuf<float> xyz;
+  DBuf<uint64_t> off;
+  DBuf<CloudInfo> ci;
+  DBuf<uint32_t> mn, mx, bucket, hist;
+  DBuf<float4> tmp;
+  DBuf<float4> pts;
+  DBuf<uint32_t> sos, vcloud, vtet, loc;
+  DBuf<uint8_t> bigflag;
+  DBuf<uint4> tv, tn, nslot;
+  DBuf<unsigned long long> ccav, cring, vote;
+  DBuf<uint32_t> centry, active, active_next, cand, cand_off, cand_len, cand_base, pool, big, freed_a, freed_b;
+  DBuf<uint8_t> st1, st2;
+  DBuf<uint64_t> lvl_off;
+  DBuf<Counters> ctr;
+  DBuf<uint32_t> ccount, hullcnt, cfill, newid;
+  DBuf<uint2> hull;
+  DBuf<uint64_t> coff;
+  DBuf<uint32_t> out_t, out_a;
+  std::vector<DBuf<uint32_t>> scan_tmp;
+  Counters* h_ctr = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int device = -1;
+
+  ~Workspace() {
+    // Released explicitly by release_thread_workspace(); CUDA may already be
+    // torn down at thread exit, so nothing is freed here.
+  }
+};
+
+namespace {
+thread_local Workspace* tl_ws = nullptr;
+
+Workspace& ws() {
+  if (!tl_ws) tl_ws = new Workspace;
+  int dev = 0;
+  ck(cudaGetDevice(&dev), "cudaGetDevice");
+  if (tl_ws->device != dev) {
+    tl_ws->device = dev;
+  }
+  if (!tl_ws->h_ctr) ck(cudaMallocHost(&tl_ws->h_ctr, sizeof(Counters)), "cudaMallocHost counters");
+  if (!tl_ws->ev0) {
+    ck(cudaEventCreate(&tl_ws->ev0), "event");
+    ck(cudaEventCreate(&tl_ws->ev1), "event");
+  }
+  return *tl_ws;
+}
+
+inline uint32_t blocks_for(uint64_t n, uint32_t threads, uint32_t cap = 148 * 16) {
+  uint64_t b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  return uint32_t(std::min<uint64_t>(b, cap));
+}
+
+}  // namespace
+
+uint64_t max_tets_for(uint64_t n) { return 8 * n + 64; }
+
+float* ws_input(size_t nfloats) {
+  Workspace& W = ws();
+  W.xyz.reserve(nfloats, "input");
+  return W.xyz.p;
+}
+
+void ws_outputs(size_t rows, uint32_t** t, uint32_t** a) {
+  Workspace& W = ws();
+  W.out_t.reserve(4 * rows, "output tets");
+  W.out_a.reserve(4 * rows, "output adjacency");
+  *t = W.out_t.p;
+  *a = W.out_a.p;
+}
+
+void release_thread_workspace() {
+  if (!tl_ws) return;
+  Workspace& w = *tl_ws;
+  w.xyz.release(); w.off.release(); w.ci.release(); w.mn.release(); w.mx.release();
+  w.bucket.release(); w.hist.release(); w.tmp.release(); w.pts.release(); w.sos.release();
+  w.vcloud.release(); w.vtet.release(); w.loc.release(); w.bigflag.release(); w.tv.release();
+  w.tn.release(); w.nslot.release(); w.ccav.release(); w.cring.release(); w.vote.release();
+  w.centry.release(); w.active.release(); w.active_next.release(); w.cand.release();
+  w.cand_off.release(); w.cand_len.release(); w.cand_base.release(); w.st1.release(); w.st2.release(); w.pool.release(); w.big.release();
+  w.freed_a.release(); w.freed_b.release(); w.lvl_off.release(); w.ctr.release();
+  w.ccount.release(); w.hullcnt.release(); w.cfill.release(); w.newid.release();
+  w.hull.release(); w.coff.release(); w.out_t.release(); w.out_a.release();
+  for (auto& b : w.scan_tmp) b.release();
+  if (w.h_ctr) cudaFreeHost(w.h_ctr);
+  if (w.ev0) cudaEventDestroy(w.ev0);
+  if (w.ev1) cudaEventDestroy(w.ev1);
+  delete tl_ws;
+  tl_ws = nullptr;
+}
+
+// Kernels with deep exact-arithmetic call chains need a few KB of stack per
+// thread.  Reserving it once keeps the driver from re-growing local memory on
+// every launch.
+void reserve_stack_once() {
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  ck(cudaGetDevice(&dev), "cudaGetDevice");
+  std::lock_guard<std::mutex> g(mu);
+  if (dev < 0 || dev >= 64 || done[dev]) return;
+  size_t need = 0;
+  const void* ks[] = {(const void*)k_expand, (const void*)k_expand_big, (const void*)k_shared,
+                      (const void*)k_relocate, (const void*)k_activate, (const void*)k_init_clouds};
+  for (const void* k : ks) {
+    cudaFuncAttributes a{};
+    if (cudaFuncGetAttributes(&a, k) == cudaSuccess) need = std::max<size_t>(need, a.localSizeBytes);
+  }
+  size_t cur = 0;
+  cudaDeviceGetLimit(&cur, cudaLimitStackSize);
+  size_t want = std::max<size_t>(need + 256, 4096);
+  if (cur < want) ck(cudaDeviceSetLimit(cudaLimitStackSize, want), "cudaDeviceSetLimit(stack)");
+  done[dev] = true;
+}
+
+JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t capacity) {
+  reserve_stack_once();
+  Workspace& W = ws();
+  cudaStream_t s = job.stream;
+  const uint32_t nc = uint32_t(job.offsets.size() - 1);
+  const uint64_t n = job.offsets.back();
+  if (n + 5ull * nc >= 0x7FFFFFF0ull) throw Error{WTET_ERR_ARG, "too many points for 31-bit vertex ids"};
+  JobResult res;
+  ck(cudaEventRecord(W.ev0, s), "event record");
+
+  // ---- per-cloud layout (host) ----
+  std::vector<CloudInfo> ci(nc);
+  uint64_t buckets = 0;
+  uint32_t maxtop = 0;
+  for (uint32_t c = 0; c < nc; ++c) {
+    uint64_t nn = job.offsets[c + 1] - job.offsets[c];
+    if (nn < 4) throw Error{WTET_ERR_ARG, "Need at least 4 points for 3D Delaunay"};
+    CloudInfo& C = ci[c];
+    C.off = job.offsets[c];
+    C.n = uint32_t(nn);
+    C.vbase = uint32_t(job.offsets[c] + 4ull * c);
+    uint32_t lg = 0;
+    while ((2ull << lg) <= nn) ++lg;  // floor(log2 n)
+    C.bbits = std::max<uint32_t>(1, std::min<uint32_t>(10, lg / 3));
+    C.bbase = uint32_t(buckets);
+    buckets += 1ull << (3 * C.bbits);
+    C.top = initial_stride_log2(nn);
+    maxtop = std::max(maxtop, C.top);
+  }
+  const uint64_t nv = n + 4ull * nc;
+  uint64_t cap0 = 0;
+  for (uint32_t c = 0; c < nc; ++c) cap0 += uint64_t(ci[c].n) * 9 / 2 * 2 + 64;  // ~9 n
+  cap0 = std::min<uint64_t>(cap0, 0x7FFFFFF0ull);
+
+  W.off.reserve(nc + 1, "offsets");
+  W.ci.reserve(nc, "clouds");
+  W.mn.reserve(3ull * nc, "bbox");
+  W.mx.reserve(3ull * nc, "bbox");
+  W.bucket.reserve(n, "bucket");
+  W.hist.reserve(buckets + 1, "hist");
+  W.tmp.reserve(n, "tmp");
+  W.pts.reserve(nv, "pts");
+  W.sos.reserve(nv, "sos");
+  W.vcloud.reserve(nv, "vcloud");
+  W.vtet.reserve(nv, "vtet");
+  W.loc.reserve(nv, "loc");
+  W.bigflag.reserve(nv, "bigflag");
+  W.centry.reserve(nc, "centry");
+  W.active.reserve(n, "active");
+  W.active_next.reserve(n, "active");
+  W.cand.reserve(n, "cand");
+  W.cand_off.reserve(n, "cand");
+  W.cand_len.reserve(n, "cand");
+  W.cand_base.reserve(n, "cand");
+  W.st1.reserve(nv, "status");
+  W.st2.reserve(nv, "status");
+  const uint32_t pool_cap = uint32_t(std::min<uint64_t>(std::max<uint64_t>(n * 24, 1 << 16), 1ull << 30));
+  W.pool.reserve(pool_cap, "pool");
+  W.big.reserve(size_t(BIG_SLOTS) * BIG_CAP, "big");
+  W.ctr.reserve(1, "counters");
+  W.lvl_off.reserve(size_t(maxtop + 1) * (nc + 1), "levels");
+  W.ccount.reserve(nc, "ccount");
+  W.hullcnt.reserve(nc, "hull");
+  W.cfill.reserve(nc, "cfill");
+  W.hull.reserve(4ull * nc, "hull");
+  W.coff.reserve(nc + 1, "coff");
+  auto reserve_tets = [&](uint64_t cap) {
+    W.tv.reserve(cap, "tv");
+    W.tn.reserve(cap, "tn");
+    W.nslot.reserve(cap, "nslot");
+    W.ccav.reserve(cap, "ccav");
+    W.cring.reserve(cap, "cring");
+    W.vote.reserve(cap, "vote");
+    W.freed_a.reserve(cap, "freed");
+    W.freed_b.reserve(cap, "freed");
+    W.newid.reserve(cap, "newid");
+  };
+  reserve_tets(cap0);
+  uint64_t cap = cap0;
+
+  ck(cudaMemcpyAsync(W.off.p, job.offsets.data(), (nc + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s), "h2d");
+  ck(cudaMemcpyAsync(W.ci.p, ci.data(), nc * sizeof(CloudInfo), cudaMemcpyHostToDevice, s), "h2d");
+  ck(cudaMemsetAsync(W.mn.p, 0xFF, 3ull * nc * 4, s), "memset");
+  ck(cudaMemsetAsync(W.mx.p, 0x00, 3ull * nc * 4, s), "memset");
+  ck(cudaMemsetAsync(W.hist.p, 0, (buckets + 1) * 4, s), "memset");
+  ck(cudaMemsetAsync(W.ctr.p, 0, sizeof(Counters), s), "memset");
+  ck(cudaMemsetAsync(W.tv.p, 0xFF, cap * sizeof(uint4), s), "memset");
+  ck(cudaMemsetAsync(W.ccav.p, 0xFF, cap * 8, s), "memset");
+  ck(cudaMemsetAsync(W.cring.p, 0xFF, cap * 8, s), "memset");
+  ck(cudaMemsetAsync(W.vote.p, 0, cap * 8, s), "memset");
+
+  Dev D{};
+  auto refresh = [&]() {
+    D.pts = W.pts.p; D.sos = W.sos.p; D.vcloud = W.vcloud.p; D.vtet = W.vtet.p; D.loc = W.loc.p;
+    D.bigflag = W.bigflag.p; D.tv = W.tv.p; D.tn = W.tn.p; D.ccav = W.ccav.p; D.cring = W.cring.p;
+    D.nslot = W.nslot.p; D.vote = W.vote.p; D.cap = uint32_t(cap); D.nv = uint32_t(nv); D.centry = W.centry.p;
+    D.active = W.active.p; D.active_next = W.active_next.p; D.cand = W.cand.p; D.cand_off = W.cand_off.p;
+    D.cand_len = W.cand_len.p; D.cand_base = W.cand_base.p; D.st1 = W.st1.p; D.st2 = W.st2.p; D.pool = W.pool.p; D.pool_cap = pool_cap; D.big = W.big.p;
+    D.freed_prev = W.freed_a.p; D.freed_next = W.freed_b.p; D.ctr = W.ctr.p;
+    D.rule = int(job.cfg.insertion_rule == WTET_RULE_CENTROID ? 1 : 0);
+  };
+  refresh();
+
+  // ---- normalise, Morton-bucket, scatter ----
+  const uint32_t T = 256;
+  uint32_t nb = uint32_t((n + T - 1) / T);
+  k_bbox<<<nb, T, 0, s>>>(job.d_xyz, W.off.p, nc, n, W.mn.p, W.mx.p);
+  k_normalize<<<nb, T, 0, s>>>(job.d_xyz, W.off.p, W.ci.p, nc, n, W.mn.p, W.mx.p, W.tmp.p, W.bucket.p, W.hist.p);
+  scan_u32(W.hist.p, uint32_t(buckets + 1), s, W.scan_tmp);
+  k_scatter_points<<<nb, T, 0, s>>>(W.off.p, W.ci.p, nc, n, W.tmp.p, W.bucket.p, W.hist.p, D);
+  k_init_clouds<<<(nc + 127) / 128, 128, 0, s>>>(W.ci.p, nc, D);
+  ck(cudaGetLastError(), "setup kernels");
+
+  // ---- strata table: lvl_off[L][c] = first index of cloud c in stratum L ----
+  std::vector<uint64_t> lvl(size_t(maxtop + 1) * (nc + 1));
+  std::vector<uint32_t> lvl_total(maxtop + 1);
+  for (uint32_t L = 0; L <= maxtop; ++L) {
+    uint64_t acc = 0;
+    for (uint32_t c = 0; c < nc; ++c) {
+      lvl[size_t(L) * (nc + 1) + c] = acc;
+      acc += level_count(ci[c].n, L, ci[c].top);
+    }
+    lvl[size_t(L) * (nc + 1) + nc] = acc;
+    lvl_total[L] = uint32_t(acc);
+  }
+  ck(cudaMemcpyAsync(W.lvl_off.p, lvl.data(), lvl.size() * 8, cudaMemcpyHostToDevice, s), "h2d");
+
+  uint32_t tet_top = nc;
+  uint32_t n_freed_prev = 0;
+  uint32_t round = 0;
+  wtet_stats st{};
+  // max_insert_iterations bounds the rounds of each stratum (src/types.rs:44-46).
+  const uint32_t max_rounds = std::max<uint32_t>(job.cfg.max_insert_iterations, 1u) * (maxtop + 1);
+  const char* tr = getenv("WTET_TRACE");
+  const int trace = tr ? atoi(tr) : 0;
+  cudaEvent_t tev[12];
+  if (trace >= 3)
+    for (auto& e : tev) cudaEventCreate(&e);
+  const uint32_t TB = 256;
+
+  int next_level = int(maxtop);
+  uint32_t n_active = 0, stratum_size = 0;
+  ck(cudaMemsetAsync(W.ctr.p, 0, sizeof(Counters), s), "memset");
+  for (;;) {
+    // Strata overlap: the next one is located once the uninserted points of
+    // the current one have thinned to a quarter, which keeps rounds full.
+    while (next_level >= 0 && (n_active == 0 || 4ull * n_active <= stratum_size)) {
+      const int L = next_level--;
+      const uint32_t total = lvl_total[L];
+      if (total == 0) continue;
+      k_activate<<<blocks_for(total, TB), TB, 0, s>>>(D, W.ci.p, W.lvl_off.p + size_t(L) * (nc + 1), nc,
+                                                      uint32_t(L), total, n_active);
+      n_active += total;
+      stratum_size = total;
+      ++st.strata;
+      break;
+    }
+    if (n_active == 0) break;
+    ++round;
+    if (round > max_rounds) throw Error{WTET_ERR_NO_CONVERGE, "insertion did not converge within max_insert_iterations"};
+    RoundArgs R;
+    R.stamp = (unsigned long long)(~round) << 32;
+    R.round = round;
+    R.n_active = n_active;
+    R.n_freed_prev = n_freed_prev;
+    R.tet_top = tet_top;
+    // Reset the per-round counters; walk / statistics counters accumulate.
+    ck(cudaMemsetAsync(W.ctr.p, 0, offsetof(Counters, err), s), "memset");
+    const uint32_t g = blocks_for(n_active, TB);
+    const uint32_t gc = blocks_for(n_active, 128);
+    auto mark = [&](int i) {
+      if (trace >= 3) cudaEventRecord(tev[i], s);
+    };
+    mark(0);
+    k_vote<<<g, TB, 0, s>>>(D, R);
+    mark(1);
+    k_expand<<<g, TB, 0, s>>>(D, R);
+    mark(2);
+    k_expand_big<<<g, TB, 0, s>>>(D, R);
+    mark(3);
+    k_resolve<<<gc, 128, 0, s>>>(D, R);
+    mark(4);
+    k_shared<<<gc, 128, 0, s>>>(D, R);
+    mark(5);
+    k_alloc<<<gc, 128, 0, s>>>(D, R);
+    mark(6);
+    k_write<<<gc, 128, 0, s>>>(D, R);
+    mark(7);
+    k_relocate<<<g, TB, 0, s>>>(D, R);
+    mark(8);
+    ck(cudaMemcpyAsync(W.h_ctr, W.ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, s), "d2h");
+    ck(cudaStreamSynchronize(s), "round");
+    Counters h = *W.h_ctr;
+    if (trace >= 3) {
+      float ms[8];
+      for (int i = 0; i < 8; ++i) cudaEventElapsedTime(&ms[i], tev[i], tev[i + 1]);
+      fprintf(stderr, "[wtet-ms] round %u vote %.3f expand %.3f big %.3f resolve %.3f shared %.3f alloc %.3f write %.3f reloc %.3f\n",
+              round, ms[0], ms[1], ms[2], ms[3], ms[4], ms[5], ms[6], ms[7]);
+    }
+    if (trace >= 2 && n_active <= 64) {
+      std::vector<uint32_t> act(n_active);
+      cudaMemcpy(act.data(), W.active.p, n_active * 4, cudaMemcpyDeviceToHost);
+      for (uint32_t a : act) {
+        float4 q;
+        uint32_t l;
+        cudaMemcpy(&q, W.pts.p + a, sizeof(float4), cudaMemcpyDeviceToHost);
+        cudaMemcpy(&l, W.loc.p + a, 4, cudaMemcpyDeviceToHost);
+        fprintf(stderr, "[wtet-pt] round %u p %u loc %u xyz %.6f %.6f %.6f\n", round, a, l, q.x, q.y, q.z);
+      }
+    }
+    if (trace)
+      fprintf(stderr, "[wtet] round %u active %u expanded %llu cand %u inserted %u big %llu alloc %u freed %u top %u err %x\n",
+              round, n_active, (unsigned long long)h.n_expanded, h.n_cand, h.n_inserted,
+              (unsigned long long)h.n_big, h.alloc_used, h.n_freed_next, tet_top, h.err);
+    if (h.err & ~uint32_t(kErrCapacity)) {
+      char buf[160];
+      snprintf(buf, sizeof buf, "device consistency check failed (flags 0x%x) in round %u", h.err, round);
+      throw Error{(h.err & kErrPrec) ? WTET_ERR_PRECISION : WTET_ERR_INTERNAL, buf};
+    }
+    st.inserted += h.n_inserted;
+    // Slots: recycled ones not handed out carry over; fresh ones extend the top.
+    uint32_t used = h.alloc_used;
+    uint32_t fresh = used > n_freed_prev ? used - n_freed_prev : 0u;
+    uint32_t left = n_freed_prev > used ? n_freed_prev - used : 0u;
+    if (left)
+      ck(cudaMemcpyAsync(W.freed_b.p + h.n_freed_next, W.freed_a.p + used, size_t(left) * 4,
+                         cudaMemcpyDeviceToDevice, s),
+         "freed carry");
+    tet_top += fresh;
+    n_freed_prev = h.n_freed_next + left;
+    std::swap(W.freed_a, W.freed_b);
+    std::swap(W.active, W.active_next);
+    n_active = h.n_next;
+    if (h.err & kErrCapacity) {
+      // Grow the tet arrays (keeping contents); the displaced winners retry.
+      uint64_t ncap = std::min<uint64_t>(cap * 3 / 2 + 1024, 0x7FFFFFF0ull);
+      if (ncap <= cap) throw Error{WTET_ERR_CAPACITY, "tet capacity exhausted"};
+      W.tv.grow_keep(ncap, tet_top, s, "grow tv");
+      ck(cudaMemsetAsync(W.tv.p + tet_top, 0xFF, (ncap - tet_top) * sizeof(uint4), s), "memset");
+      W.tn.grow_keep(ncap, tet_top, s, "grow tn");
+      W.nslot.grow_keep(ncap, 0, s, "grow nslot");
+      W.ccav.grow_keep(ncap, tet_top, s, "grow ccav");
+      ck(cudaMemsetAsync(W.ccav.p + tet_top, 0xFF, (ncap - tet_top) * 8, s), "memset");
+      W.cring.grow_keep(ncap, tet_top, s, "grow cring");
+      ck(cudaMemsetAsync(W.cring.p + tet_top, 0xFF, (ncap - tet_top) * 8, s), "memset");
+      W.vote.grow_keep(ncap, tet_top, s, "grow vote");
+      ck(cudaMemsetAsync(W.vote.p + tet_top, 0, (ncap - tet_top) * 8, s), "memset");
+      W.freed_a.grow_keep(ncap, n_freed_prev, s, "grow freed");
+      W.freed_b.grow_keep(ncap, 0, s, "grow freed");
+      W.newid.grow_keep(ncap, 0, s, "grow newid");
+      cap = ncap;
+      uint32_t zero = 0;
+      ck(cudaMemcpyAsync(&W.ctr.p->err, &zero, 4, cudaMemcpyHostToDevice, s), "clear err");
+      ck(cudaStreamSynchronize(s), "grow");
+    }
+    refresh();
+    D.freed_prev = W.freed_a.p;
+    D.freed_next = W.freed_b.p;
+    D.active = W.active.p;
+    D.active_next = W.active_next.p;
+  }
+  st.walk_steps = W.h_ctr->walk_steps;
+  st.candidates = W.h_ctr->n_expanded;
+  st.big_cavities = W.h_ctr->n_big;
+  st.tets_created = W.h_ctr->created;
+  st.rounds = round;
+
+  // ---- output: per-cloud numbering, rows, infinity tets ----
+  ck(cudaMemsetAsync(W.ccount.p, 0, nc * 4, s), "memset");
+  ck(cudaMemsetAsync(W.hullcnt.p, 0, nc * 4, s), "memset");
+  ck(cudaMemsetAsync(W.cfill.p, 0, nc * 4, s), "memset");
+  uint32_t gt = blocks_for(tet_top, TB, 148 * 32);
+  k_count<<<gt, TB, 0, s>>>(D, tet_top, W.ccount.p, W.hullcnt.p, W.hull.p);
+  std::vector<uint32_t> ccount(nc);
+  ck(cudaMemcpyAsync(ccount.data(), W.ccount.p, nc * 4, cudaMemcpyDeviceToHost, s), "d2h");
+  ck(cudaStreamSynchronize(s), "count");
+  res.tet_offsets.resize(nc + 1);
+  uint64_t acc = 0;
+  for (uint32_t c = 0; c < nc; ++c) {
+    res.tet_offsets[c] = acc;
+    acc += uint64_t(ccount[c]) + 4;
+  }
+  res.tet_offsets[nc] = acc;
+  st.num_tets = acc;
+  if (d_out_t && d_out_a && acc <= capacity) {
+    ck(cudaMemcpyAsync(W.coff.p, res.tet_offsets.data(), (nc + 1) * 8, cudaMemcpyHostToDevice, s), "h2d");
+    k_number<<<gt, TB, 0, s>>>(D, tet_top, W.cfill.p, W.newid.p);
+    k_emit<<<gt, TB, 0, s>>>(D, tet_top, W.newid.p, W.coff.p, d_out_t, d_out_a);
+    k_infinity<<<(nc + 127) / 128, 128, 0, s>>>(D, W.ci.p, nc, W.ccount.p, W.hullcnt.p, W.hull.p, W.newid.p,
+                                                W.coff.p, d_out_t, d_out_a);
+    ck(cudaGetLastError(), "output kernels");
+  }
+  ck(cudaEventRecord(W.ev1, s), "event record");
+  ck(cudaMemcpyAsync(W.h_ctr, W.ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, s), "d2h");
+  ck(cudaStreamSynchronize(s), "output");
+  if (W.h_ctr->err) {
+    char buf[128];
+    snprintf(buf, sizeof buf, "device consistency check failed in output (flags 0x%x)", W.h_ctr->err);
+    throw Error{WTET_ERR_INTERNAL, buf};
+  }
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, W.ev0, W.ev1);
+  st.device_ms = ms;
+  res.stats = st;
+  return res;
+}
+
+// ------------------------------------------------------- quality check ----
+
+__global__ void k_check_quality(const float4* pts, uint32_t n, const uint4* tets, const uint4* adj, uint64_t m,
+                                unsigned long long* out, uint32_t* err) {
+  unsigned long long viol = 0, interior = 0;
+  for (uint64_t ti = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; ti < m; ti += uint64_t(gridDim.x) * blockDim.x) {
+    uint4 t = tets[ti];
+    if (t.x >= n || t.y >= n || t.z >= n || t.w >= n) continue;
+    ++interior;
+    uint4 a = adj[ti];
+    for (int f = 0; f < 4; ++f) {
+      uint32_t packed = comp(a, f);
+      if (packed == NONE) continue;
+      uint64_t oti = packed >> 5;
+      uint32_t of = packed & 3;
+      if (ti >= oti) continue;
+      if (oti >= m) {
+        atomicOr(err, 1u);
+        continue;
+      }
+      uint4 o = tets[oti];
+      if (o.x >= n || o.y >= n || o.z >= n || o.w >= n) continue;
+      uint32_t vb = comp(o, of);
+      double P[5][3];
+      load_pt(pts, t.x, P[0]);
+      load_pt(pts, t.y, P[1]);
+      load_pt(pts, t.z, P[2]);
+      load_pt(pts, t.w, P[3]);
+      load_pt(pts, vb, P[4]);
+      int s = ex::insphere(P[0], P[1], P[2], P[3], P[4], err);
+      if (s == 0) {
+        // SoS keys are the input indices themselves.
+        s = ex::orient4d_sos_degenerate(P[0], P[1], P[2], P[3], P[4], t.x, t.y, t.z, t.w, vb, err);
+      }
+      if (s < 0) ++viol;
+    }
+  }
+  atomicAdd(&out[0], viol);
+  atomicAdd(&out[1], interior);
+}
+
+__global__ void k_normalize_plain(const float* xyz, uint64_t n, const uint32_t* mn, const uint32_t* mx, float4* out) {
+  uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float lo[3], ext[3];
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = o2f(mn[k]);
+    ext[k] = o2f(mx[k]) - lo[k];
+  }
+  float s = fmaxf(fmaxf(fmaxf(ext[0], ext[1]), ext[2]), 1e-10f);
+  out[i] = make_float4(__fdiv_rn(__fsub_rn(xyz[3 * i], lo[0]), s), __fdiv_rn(__fsub_rn(xyz[3 * i + 1], lo[1]), s),
+                       __fdiv_rn(__fsub_rn(xyz[3 * i + 2], lo[2]), s), 0.f);
+}
+
+void check_quality_device(const float* d_xyz, uint64_t n, const uint32_t* d_tets, const uint32_t* d_adj, uint64_t m,
+                          uint64_t* violations, uint64_t* interior, cudaStream_t s) {
+  Workspace& W = ws();
+  W.off.reserve(2, "off");
+  W.mn.reserve(3, "bbox");
+  W.mx.reserve(3, "bbox");
+  W.tmp.reserve(n, "tmp");
+  W.ctr.reserve(1, "ctr");
+  uint64_t offs[2] = {0, n};
+  ck(cudaMemcpyAsync(W.off.p, offs, 16, cudaMemcpyHostToDevice, s), "h2d");
+  ck(cudaMemsetAsync(W.mn.p, 0xFF, 12, s), "memset");
+  ck(cudaMemsetAsync(W.mx.p, 0, 12, s), "memset");
+  ck(cudaMemsetAsync(W.ctr.p, 0, sizeof(Counters), s), "memset");
+  uint32_t nb = uint32_t((n + 255) / 256);
+  k_bbox<<<nb, 256, 0, s>>>(d_xyz, W.off.p, 1, n, W.mn.p, W.mx.p);
+  k_normalize_plain<<<nb, 256, 0, s>>>(d_xyz, n, W.mn.p, W.mx.p, W.tmp.p);
+  unsigned long long* out = reinterpret_cast<unsigned long long*>(&W.ctr.p->walk_steps);
+  k_check_quality<<<blocks_for(m, 128, 148 * 16), 128, 0, s>>>(W.tmp.p, uint32_t(n), reinterpret_cast<const uint4*>(d_tets),
+                                                                reinterpret_cast<const uint4*>(d_adj), m, out,
+                                                                &W.ctr.p->err);
+  ck(cudaMemcpyAsync(W.h_ctr, W.ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, s), "d2h");
+  ck(cudaStreamSynchronize(s), "check");
+  if (W.h_ctr->err & ~uint32_t(kErrPrec))
+    throw Error{WTET_ERR_ARG, "adjacency refers to a tet out of range"};
+  if (W.h_ctr->err & kErrPrec) throw Error{WTET_ERR_PRECISION, "exact arithmetic buffer overflow"};
+  *violations = W.h_ctr->walk_steps;
+  *interior = W.h_ctr->n_expanded;
+}
+
+}  // namespace wtet

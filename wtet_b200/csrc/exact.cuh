@@ -1,0 +1,561 @@
+// Exact geometric predicates on the device: an FP64 static filter, an FP64
+// expansion-arithmetic exact stage built from two-sum / two-product, then
+// Simulation of Simplicity with the reference's cascades.
+//
+//   orient3d / insphere signs   src/predicates.rs:14-21 (Shewchuk semantics)
+//   orient3d_sos                src/predicates.rs:106-208
+//   orient4d (insphere + SoS)   src/predicates.rs:450-675
+//
+// Coordinates are f32 values widened to f64.  The exact stage evaluates the
+// determinants from raw coordinates (4x4 / 5x5 with a column of ones, expanded
+// by cofactors), so it needs no exact coordinate differences.  The SoS
+// cascades reproduce the reference's arithmetic operation by operation,
+// including its plain-double orient2d and coordinate differences and its own
+// filtered lifted orient3d; this file must be compiled with -fmad=false so
+// that every product and sum is rounded on its own, as in the reference.
+#pragma once
+#include <cstdint>
+
+namespace wtet {
+namespace ex {
+
+// Error flag bit raised when an expansion would outgrow its fixed buffer.
+constexpr uint32_t kErrPrecision = 1u << 4;
+
+struct ErrSink {
+  uint32_t* flags;
+};
+
+__device__ __forceinline__ void raise_precision(uint32_t* flags) {
+  if (flags) atomicOr(flags, kErrPrecision);
+}
+
+__device__ __forceinline__ void two_sum(double a, double b, double& x, double& y) {
+  x = a + b;
+  double bv = x - a;
+  double av = x - bv;
+  y = (a - av) + (b - bv);
+}
+__device__ __forceinline__ void fast_two_sum(double a, double b, double& x, double& y) {
+  x = a + b;
+  y = b - (x - a);
+}
+// Exact product with one fused multiply-add for the rounding error.
+__device__ __forceinline__ void two_prod(double a, double b, double& x, double& y) {
+  x = a * b;
+  y = __fma_rn(a, b, -x);
+}
+
+// h = e + f with zero elimination.  Components are stored with increasing
+// magnitude; the result has at least one component.
+__device__ __noinline__ int esum(int el, const double* e, int fl, const double* f, double* h) {
+  double Q, Qn, hh;
+  double en = e[0], fn = f[0];
+  int ei = 0, fi = 0, hi = 0;
+  if ((fn > en) == (fn > -en)) {
+    Q = en;
+    en = (++ei < el) ? e[ei] : 0.0;
+  } else {
+    Q = fn;
+    fn = (++fi < fl) ? f[fi] : 0.0;
+  }
+  if (ei < el && fi < fl) {
+    if ((fn > en) == (fn > -en)) {
+      fast_two_sum(en, Q, Qn, hh);
+      en = (++ei < el) ? e[ei] : 0.0;
+    } else {
+      fast_two_sum(fn, Q, Qn, hh);
+      fn = (++fi < fl) ? f[fi] : 0.0;
+    }
+    Q = Qn;
+    if (hh != 0.0) h[hi++] = hh;
+    while (ei < el && fi < fl) {
+      if ((fn > en) == (fn > -en)) {
+        two_sum(Q, en, Qn, hh);
+        en = (++ei < el) ? e[ei] : 0.0;
+      } else {
+        two_sum(Q, fn, Qn, hh);
+        fn = (++fi < fl) ? f[fi] : 0.0;
+      }
+      Q = Qn;
+      if (hh != 0.0) h[hi++] = hh;
+    }
+  }
+  while (ei < el) {
+    two_sum(Q, en, Qn, hh);
+    en = (++ei < el) ? e[ei] : 0.0;
+    Q = Qn;
+    if (hh != 0.0) h[hi++] = hh;
+  }
+  while (fi < fl) {
+    two_sum(Q, fn, Qn, hh);
+    fn = (++fi < fl) ? f[fi] : 0.0;
+    Q = Qn;
+    if (hh != 0.0) h[hi++] = hh;
+  }
+  if (Q != 0.0 || hi == 0) h[hi++] = Q;
+  return hi;
+}
+
+// h = b * e with zero elimination.
+__device__ __noinline__ int escale(int el, const double* e, double b, double* h) {
+  double Q, s, hh, p1, p0;
+  int hi = 0;
+  two_prod(e[0], b, Q, hh);
+  if (hh != 0.0) h[hi++] = hh;
+  for (int i = 1; i < el; ++i) {
+    two_prod(e[i], b, p1, p0);
+    two_sum(Q, p0, s, hh);
+    if (hh != 0.0) h[hi++] = hh;
+    fast_two_sum(p1, s, Q, hh);
+    if (hh != 0.0) h[hi++] = hh;
+  }
+  if (Q != 0.0 || hi == 0) h[hi++] = Q;
+  return hi;
+}
+
+// In-place compression (most significant component last).
+__device__ __noinline__ int ecompress(int el, double* e) {
+  double Q = e[el - 1], q, Qn;
+  int bottom = el - 1;
+  for (int i = el - 2; i >= 0; --i) {
+    fast_two_sum(Q, e[i], Qn, q);
+    if (q != 0.0) {
+      e[bottom--] = Qn;
+      Q = q;
+    } else {
+      Q = Qn;
+    }
+  }
+  int top = 0;
+  for (int i = bottom + 1; i < el; ++i) {
+    fast_two_sum(e[i], Q, Qn, q);
+    if (q != 0.0) e[top++] = q;
+    Q = Qn;
+  }
+  e[top++] = Q;
+  return top;
+}
+
+__device__ __forceinline__ int esign(int n, const double* e) {
+  double v = e[n - 1];
+  return (v > 0.0) - (v < 0.0);
+}
+
+// p_u q_v - q_u p_v as a 4-component expansion.
+__device__ __forceinline__ int minor2(const double* p, const double* q, int u, int v, double* h) {
+  double a[2], b[2];
+  two_prod(p[u], q[v], a[1], a[0]);
+  two_prod(q[u], p[v], b[1], b[0]);
+  b[0] = -b[0];
+  b[1] = -b[1];
+  return esum(2, a, 2, b, h);
+}
+
+// det[[p_u,p_v,1],[q_u,q_v,1],[r_u,r_v,1]] (<= 12 components).
+__device__ __forceinline__ int minor3(const double* p, const double* q, const double* r, int u, int v,
+                                      double* h) {
+  double m1[4], m2[4], m3[4], t[8];
+  int l1 = minor2(p, q, u, v, m1);
+  int l2 = minor2(q, r, u, v, m2);
+  int l3 = minor2(r, p, u, v, m3);
+  int lt = esum(l1, m1, l2, m2, t);
+  return esum(lt, t, l3, m3, h);
+}
+
+// |p|^2 exactly (<= 6 components, compressed).
+__device__ __forceinline__ int lift(const double* p, double* h) {
+  double a[2], b[2], c[2], t[4];
+  two_prod(p[0], p[0], a[1], a[0]);
+  two_prod(p[1], p[1], b[1], b[0]);
+  two_prod(p[2], p[2], c[1], c[0]);
+  int lt = esum(2, a, 2, b, t);
+  int n = esum(lt, t, 2, c, h);
+  return ecompress(n, h);
+}
+
+// det4 with columns (u, v, K, 1) over rows a..d where K is an expansion per
+// row of at most 6 components.  Returns the compressed length in h (<= 32),
+// or -1 if a buffer would overflow.
+__device__ __noinline__ int det4k(const double* a, const double* b, const double* c, const double* d, int u,
+                                  int v, const int* kl, const double (*K)[6], double* h) {
+  const double* P[4] = {a, b, c, d};
+  double acc[64], tmp[64], m[12], sc[24];
+  int alen = 0;
+#pragma unroll 1
+  for (int i = 0; i < 4; ++i) {
+    const double* x = P[i == 0 ? 1 : 0];
+    const double* y = P[i <= 1 ? 2 : 1];
+    const double* z = P[i <= 2 ? 3 : 2];
+    int ml = minor3(x, y, z, u, v, m);
+    ml = ecompress(ml, m);
+#pragma unroll 1
+    for (int j = 0; j < kl[i]; ++j) {
+      double kv = (i & 1) ? -K[i][j] : K[i][j];
+      int sl = escale(ml, m, kv, sc);
+      if (alen == 0) {
+        for (int q = 0; q < sl; ++q) acc[q] = sc[q];
+        alen = sl;
+      } else {
+        if (alen + sl > 64) return -1;
+        int nl = esum(alen, acc, sl, sc, tmp);
+        nl = ecompress(nl, tmp);
+        for (int q = 0; q < nl; ++q) acc[q] = tmp[q];
+        alen = nl;
+      }
+    }
+  }
+  alen = ecompress(alen, acc);
+  if (alen > 32) return -1;
+  for (int q = 0; q < alen; ++q) h[q] = acc[q];
+  return alen;
+}
+
+// Exact Shewchuk orient3d value = det[[x,y,z,1]] rows a..d.
+__device__ __forceinline__ int orient3d_expansion(const double* a, const double* b, const double* c,
+                                                  const double* d, double* h) {
+  const int kl[4] = {1, 1, 1, 1};
+  const double K[4][6] = {{a[2]}, {b[2]}, {c[2]}, {d[2]}};
+  return det4k(a, b, c, d, 0, 1, kl, K, h);
+}
+
+__device__ __noinline__ int orient3d_exact_sign(const double* a, const double* b, const double* c,
+                                                const double* d, uint32_t* flags) {
+  double h[32];
+  int n = orient3d_expansion(a, b, c, d, h);
+  if (n < 0) {
+    raise_precision(flags);
+    return 0;
+  }
+  return esign(n, h);
+}
+
+// Exact insphere: D5 = -w_a D4(bcde) + w_b D4(acde) - w_c D4(abde) + w_d D4(abce) - w_e D4(abcd).
+__device__ __noinline__ int insphere_exact_sign(const double* a, const double* b, const double* c,
+                                                const double* d, const double* e, uint32_t* flags) {
+  const double* P[5] = {a, b, c, d, e};
+  double acc[96], tmp[96], d4[32], w[6], sc[64];
+  int alen = 0;
+#pragma unroll 1
+  for (int i = 0; i < 5; ++i) {
+    const double* q[4];
+    int k = 0;
+    for (int j = 0; j < 5; ++j)
+      if (j != i) q[k++] = P[j];
+    int dl = orient3d_expansion(q[0], q[1], q[2], q[3], d4);
+    if (dl < 0) {
+      raise_precision(flags);
+      return 0;
+    }
+    if (dl == 1 && d4[0] == 0.0) continue;
+    int wl = lift(P[i], w);
+#pragma unroll 1
+    for (int j = 0; j < wl; ++j) {
+      double wv = (i & 1) ? w[j] : -w[j];
+      int sl = escale(dl, d4, wv, sc);
+      if (alen == 0) {
+        for (int t = 0; t < sl; ++t) acc[t] = sc[t];
+        alen = sl;
+      } else {
+        if (alen + sl > 96) {
+          raise_precision(flags);
+          return 0;
+        }
+        int nl = esum(alen, acc, sl, sc, tmp);
+        nl = ecompress(nl, tmp);
+        for (int t = 0; t < nl; ++t) acc[t] = tmp[t];
+        alen = nl;
+      }
+    }
+  }
+  if (alen == 0) return 0;
+  return esign(alen, acc);
+}
+
+constexpr double kEps = 1.1102230246251565e-16;  // 2^-53
+constexpr double kO3dBoundA = (7.0 + 56.0 * kEps) * kEps;
+constexpr double kIspBoundA = (16.0 + 224.0 * kEps) * kEps;
+constexpr double kO3dBoundLifted = (11.0 + 112.0 * kEps) * kEps;  // src/predicates.rs:426-427
+
+// Sign of Shewchuk orient3d(a,b,c,d): FP64 filter, then exact.
+__device__ __forceinline__ int orient3d(const double* pa, const double* pb, const double* pc, const double* pd,
+                                        uint32_t* flags) {
+  double adx = pa[0] - pd[0], bdx = pb[0] - pd[0], cdx = pc[0] - pd[0];
+  double ady = pa[1] - pd[1], bdy = pb[1] - pd[1], cdy = pc[1] - pd[1];
+  double adz = pa[2] - pd[2], bdz = pb[2] - pd[2], cdz = pc[2] - pd[2];
+  double bdxcdy = bdx * cdy, cdxbdy = cdx * bdy;
+  double cdxady = cdx * ady, adxcdy = adx * cdy;
+  double adxbdy = adx * bdy, bdxady = bdx * ady;
+  double det = adz * (bdxcdy - cdxbdy) + bdz * (cdxady - adxcdy) + cdz * (adxbdy - bdxady);
+  double perm = (fabs(bdxcdy) + fabs(cdxbdy)) * fabs(adz) + (fabs(cdxady) + fabs(adxcdy)) * fabs(bdz) +
+                (fabs(adxbdy) + fabs(bdxady)) * fabs(cdz);
+  double err = kO3dBoundA * perm;
+  if (det > err) return 1;
+  if (-det > err) return -1;
+  return orient3d_exact_sign(pa, pb, pc, pd, flags);
+}
+
+// Sign of Shewchuk insphere(a,b,c,d,e): FP64 filter, then exact.
+__device__ __forceinline__ int insphere(const double* pa, const double* pb, const double* pc, const double* pd,
+                                        const double* pe, uint32_t* flags) {
+  double aex = pa[0] - pe[0], bex = pb[0] - pe[0], cex = pc[0] - pe[0], dex = pd[0] - pe[0];
+  double aey = pa[1] - pe[1], bey = pb[1] - pe[1], cey = pc[1] - pe[1], dey = pd[1] - pe[1];
+  double aez = pa[2] - pe[2], bez = pb[2] - pe[2], cez = pc[2] - pe[2], dez = pd[2] - pe[2];
+  double aexbey = aex * bey, bexaey = bex * aey, ab = aexbey - bexaey;
+  double bexcey = bex * cey, cexbey = cex * bey, bc = bexcey - cexbey;
+  double cexdey = cex * dey, dexcey = dex * cey, cd = cexdey - dexcey;
+  double dexaey = dex * aey, aexdey = aex * dey, da = dexaey - aexdey;
+  double aexcey = aex * cey, cexaey = cex * aey, ac = aexcey - cexaey;
+  double bexdey = bex * dey, dexbey = dex * bey, bd = bexdey - dexbey;
+  double abc = aez * bc - bez * ac + cez * ab;
+  double bcd = bez * cd - cez * bd + dez * bc;
+  double cda = cez * da + dez * ac + aez * cd;
+  double dab = dez * ab + aez * bd + bez * da;
+  double alift = aex * aex + aey * aey + aez * aez;
+  double blift = bex * bex + bey * bey + bez * bez;
+  double clift = cex * cex + cey * cey + cez * cez;
+  double dlift = dex * dex + dey * dey + dez * dez;
+  double det = (dlift * abc - clift * dab) + (blift * cda - alift * bcd);
+  double az = fabs(aez), bz = fabs(bez), cz = fabs(cez), dz = fabs(dez);
+  double p_ab = fabs(aexbey) + fabs(bexaey), p_bc = fabs(bexcey) + fabs(cexbey);
+  double p_cd = fabs(cexdey) + fabs(dexcey), p_da = fabs(dexaey) + fabs(aexdey);
+  double p_ac = fabs(aexcey) + fabs(cexaey), p_bd = fabs(bexdey) + fabs(dexbey);
+  double perm = (p_cd * bz + p_bd * cz + p_bc * dz) * alift + (p_da * cz + p_ac * dz + p_cd * az) * blift +
+                (p_ab * dz + p_bd * az + p_da * bz) * clift + (p_bc * az + p_ac * bz + p_ab * cz) * dlift;
+  double err = kIspBoundA * perm;
+  if (det > err) return 1;
+  if (-det > err) return -1;
+  return insphere_exact_sign(pa, pb, pc, pd, pe, flags);
+}
+
+// ---- SoS cascade pieces (src/predicates.rs) ----
+
+// Plain double orient2d on coordinates (u, v): src/predicates.rs:73-75.
+__device__ __forceinline__ double orient2d_plain(const double* a, const double* b, const double* c, int u,
+                                                 int v) {
+  return (a[u] - c[u]) * (b[v] - c[v]) - (a[v] - c[v]) * (b[u] - c[u]);
+}
+
+// Lifted orient3d on permuted coordinates: the reference's filter and error
+// bound (src/predicates.rs:390-435), then the exact sign of det[[u,v,|p|^2,1]].
+__device__ __noinline__ int orient3d_lifted(const double* a0, const double* b0, const double* c0,
+                                            const double* d0, int q0, int q1, int q2, uint32_t* flags) {
+  double pa[3] = {a0[q0], a0[q1], a0[q2]};
+  double pb[3] = {b0[q0], b0[q1], b0[q2]};
+  double pc[3] = {c0[q0], c0[q1], c0[q2]};
+  double pd[3] = {d0[q0], d0[q1], d0[q2]};
+  double adx = pa[0] - pd[0], bdx = pb[0] - pd[0], cdx = pc[0] - pd[0];
+  double ady = pa[1] - pd[1], bdy = pb[1] - pd[1], cdy = pc[1] - pd[1];
+  double adzr = pa[2] - pd[2], bdzr = pb[2] - pd[2], cdzr = pc[2] - pd[2];
+  double adz = adx * adx + ady * ady + adzr * adzr;
+  double bdz = bdx * bdx + bdy * bdy + bdzr * bdzr;
+  double cdz = cdx * cdx + cdy * cdy + cdzr * cdzr;
+  double bdxcdy = bdx * cdy, cdxbdy = cdx * bdy, cdxady = cdx * ady;
+  double adxcdy = adx * cdy, adxbdy = adx * bdy, bdxady = bdx * ady;
+  double det = adz * (bdxcdy - cdxbdy) + bdz * (cdxady - adxcdy) + cdz * (adxbdy - bdxady);
+  double perm = (fabs(bdxcdy) + fabs(cdxbdy)) * fabs(adz) + (fabs(cdxady) + fabs(adxcdy)) * fabs(bdz) +
+                (fabs(adxbdy) + fabs(bdxady)) * fabs(cdz);
+  double err = kO3dBoundLifted * perm;
+  if (det > err || -det > err) return (det > 0.0) - (det < 0.0);
+  int kl[4];
+  double K[4][6];
+  kl[0] = lift(pa, K[0]);
+  kl[1] = lift(pb, K[1]);
+  kl[2] = lift(pc, K[2]);
+  kl[3] = lift(pd, K[3]);
+  double h[32];
+  int n = det4k(pa, pb, pc, pd, 0, 1, kl, K, h);
+  if (n < 0) {
+    raise_precision(flags);
+    return 0;
+  }
+  return esign(n, h);
+}
+
+// Exact sign of a_u (w_b - w_c) + b_u (w_c - w_a) + c_u (w_a - w_b): src/predicates.rs:255-291.
+__device__ __noinline__ int orient2d_lifted(const double* a, const double* b, const double* c, int q0) {
+  double W[3][6];
+  int L[3];
+  L[0] = lift(a, W[0]);
+  L[1] = lift(b, W[1]);
+  L[2] = lift(c, W[2]);
+  const double U[3] = {a[q0], b[q0], c[q0]};
+  double acc[80], tmp[80], sc[12];
+  int alen = 0;
+#pragma unroll 1
+  for (int i = 0; i < 3; ++i) {
+#pragma unroll 1
+    for (int s = 0; s < 2; ++s) {
+      int j = (i + 1 + s) % 3;
+      int sl = escale(L[j], W[j], s == 0 ? U[i] : -U[i], sc);
+      if (alen == 0) {
+        for (int t = 0; t < sl; ++t) acc[t] = sc[t];
+        alen = sl;
+      } else {
+        int nl = esum(alen, acc, sl, sc, tmp);
+        nl = ecompress(nl, tmp);
+        for (int t = 0; t < nl; ++t) acc[t] = tmp[t];
+        alen = nl;
+      }
+    }
+  }
+  return esign(alen, acc);
+}
+
+// Exact sign of |a|^2 - |b|^2: src/predicates.rs:229-252.
+__device__ __noinline__ int orient1d_lifted(const double* a, const double* b) {
+  double wa[6], wb[6], h[12];
+  int la = lift(a, wa), lb = lift(b, wb);
+  for (int i = 0; i < lb; ++i) wb[i] = -wb[i];
+  int n = esum(la, wa, lb, wb, h);
+  return esign(n, h);
+}
+
+// One level of the orient4d SoS cascade (src/predicates.rs:513-667): term
+// kind, the sorted points used, coordinate permutation, sign flip.
+enum : uint8_t { kO3 = 0, kO3L, kO2, kO2L, kO1, kO1L, kConst };
+struct SosLevel {
+  uint8_t kind, p0, p1, p2, p3, q0, q1, q2, flip;
+};
+
+__constant__ SosLevel kSos4[49] = {
+    {kO3, 1, 2, 3, 4, 0, 1, 2, 1},  {kO3L, 1, 2, 3, 4, 0, 1, 2, 0}, {kO3L, 1, 2, 3, 4, 0, 2, 1, 1},
+    {kO3L, 1, 2, 3, 4, 1, 2, 0, 0}, {kO3, 0, 2, 3, 4, 0, 1, 2, 0},  {kO2, 2, 3, 4, 0, 0, 1, 2, 0},
+    {kO2, 2, 3, 4, 0, 0, 2, 1, 1},  {kO2, 2, 3, 4, 0, 1, 2, 0, 0},  {kO3L, 0, 2, 3, 4, 0, 1, 2, 1},
+    {kO2L, 2, 3, 4, 0, 0, 1, 2, 0}, {kO2L, 2, 3, 4, 0, 1, 0, 2, 1}, {kO3L, 0, 2, 3, 4, 0, 2, 1, 0},
+    {kO2L, 2, 3, 4, 0, 2, 0, 1, 0}, {kO3L, 0, 2, 3, 4, 1, 2, 0, 1}, {kO3, 0, 1, 3, 4, 0, 1, 2, 1},
+    {kO2, 1, 3, 4, 0, 0, 1, 2, 1},  {kO2, 1, 3, 4, 0, 0, 2, 1, 0},  {kO2, 1, 3, 4, 0, 1, 2, 0, 1},
+    {kO2, 0, 3, 4, 0, 0, 1, 2, 0},  {kO1, 3, 4, 0, 0, 0, 1, 2, 1},  {kO1, 3, 4, 0, 0, 1, 0, 2, 0},
+    {kO2, 0, 3, 4, 0, 0, 2, 1, 1},  {kO1, 3, 4, 0, 0, 2, 0, 1, 1},  {kO2, 0, 3, 4, 0, 1, 2, 0, 0},
+    {kO3L, 0, 1, 3, 4, 0, 1, 2, 0}, {kO2L, 1, 3, 4, 0, 0, 1, 2, 1}, {kO2L, 1, 3, 4, 0, 1, 0, 2, 0},
+    {kO2L, 0, 3, 4, 0, 0, 1, 2, 0}, {kO1L, 3, 4, 0, 0, 0, 1, 2, 0}, {kO2L, 0, 3, 4, 0, 1, 0, 2, 1},
+    {kO3L, 0, 1, 3, 4, 0, 2, 1, 1}, {kO2L, 1, 3, 4, 0, 2, 0, 1, 1}, {kO2L, 0, 3, 4, 0, 2, 0, 1, 0},
+    {kO3L, 0, 1, 3, 4, 1, 2, 0, 0}, {kO3, 0, 1, 2, 4, 0, 1, 2, 0},  {kO2, 1, 2, 4, 0, 0, 1, 2, 0},
+    {kO2, 1, 2, 4, 0, 0, 2, 1, 1},  {kO2, 1, 2, 4, 0, 1, 2, 0, 0},  {kO2, 0, 2, 4, 0, 0, 1, 2, 1},
+    {kO1, 2, 4, 0, 0, 0, 1, 2, 0},  {kO1, 2, 4, 0, 0, 1, 0, 2, 1},  {kO2, 0, 2, 4, 0, 0, 2, 1, 0},
+    {kO1, 2, 4, 0, 0, 2, 0, 1, 0},  {kO2, 0, 2, 4, 0, 1, 2, 0, 1},  {kO2, 0, 1, 4, 0, 0, 1, 2, 0},
+    {kO1, 1, 4, 0, 0, 0, 1, 2, 1},  {kO1, 1, 4, 0, 0, 1, 0, 2, 0},  {kO1, 0, 4, 0, 0, 0, 1, 2, 0},
+    {kConst, 0, 0, 0, 0, 0, 1, 2, 0},
+};
+
+// Sorts (key, point) pairs by key with insertion sort; returns parity.
+template <int N>
+__device__ __forceinline__ int sort_keys(uint32_t* k, const double** p) {
+  int parity = 0;
+#pragma unroll
+  for (int i = 1; i < N; ++i) {
+#pragma unroll
+    for (int j = i; j > 0; --j) {
+      if (k[j] < k[j - 1]) {
+        uint32_t tk = k[j];
+        k[j] = k[j - 1];
+        k[j - 1] = tk;
+        const double* tp = p[j];
+        p[j] = p[j - 1];
+        p[j - 1] = tp;
+        parity ^= 1;
+      }
+    }
+  }
+  return parity;
+}
+
+// gDel3D orientation with SoS: +1 iff the exact det < 0; never 0.
+__device__ __noinline__ int orient3d_sos_degenerate(const double* a, const double* b, const double* c,
+                                                    const double* d, uint32_t ia, uint32_t ib, uint32_t ic,
+                                                    uint32_t id) {
+  uint32_t k[4] = {ia, ib, ic, id};
+  const double* p[4] = {a, b, c, d};
+  int parity = sort_keys<4>(k, p);
+  double r = 1.0;
+  int depth = 13;
+#pragma unroll 1
+  for (int dd = 0; dd < 13; ++dd) {
+    double v;
+    switch (dd) {
+      case 0: v = orient2d_plain(p[1], p[2], p[3], 0, 1); break;
+      case 1: v = orient2d_plain(p[1], p[2], p[3], 0, 2); break;
+      case 2: v = orient2d_plain(p[1], p[2], p[3], 1, 2); break;
+      case 3: v = orient2d_plain(p[0], p[2], p[3], 0, 1); break;
+      case 4: v = p[2][0] - p[3][0]; break;
+      case 5: v = p[2][1] - p[3][1]; break;
+      case 6: v = orient2d_plain(p[0], p[2], p[3], 0, 2); break;
+      case 7: v = p[2][2] - p[3][2]; break;
+      case 8: v = orient2d_plain(p[0], p[2], p[3], 1, 2); break;
+      case 9: v = orient2d_plain(p[0], p[1], p[3], 0, 1); break;
+      case 10: v = p[1][0] - p[3][0]; break;
+      case 11: v = p[1][1] - p[3][1]; break;
+      default: v = p[0][0] - p[3][0]; break;
+    }
+    if (v != 0.0) {
+      r = v;
+      depth = dd;
+      break;
+    }
+  }
+  int sg = (r > 0.0) - (r < 0.0);
+  if (depth == 1 || depth == 3 || depth == 5 || depth == 8 || depth == 10) sg = -sg;
+  if (parity) sg = -sg;
+  return sg < 0 ? 1 : -1;
+}
+
+__device__ __forceinline__ int orient3d_sos(const double* a, const double* b, const double* c, const double* d,
+                                            uint32_t ia, uint32_t ib, uint32_t ic, uint32_t id,
+                                            uint32_t* flags) {
+  int s = orient3d(a, b, c, d, flags);
+  if (s != 0) return s < 0 ? 1 : -1;
+  return orient3d_sos_degenerate(a, b, c, d, ia, ib, ic, id);
+}
+
+__device__ __noinline__ int orient4d_sos_degenerate(const double* a, const double* b, const double* c,
+                                                    const double* d, const double* e, uint32_t ia, uint32_t ib,
+                                                    uint32_t ic, uint32_t id, uint32_t ie, uint32_t* flags) {
+  uint32_t k[5] = {ia, ib, ic, id, ie};
+  const double* p[5] = {a, b, c, d, e};
+  int parity = sort_keys<5>(k, p);
+  int sg = 1;
+#pragma unroll 1
+  for (int lv = 0; lv < 49; ++lv) {
+    const SosLevel L = kSos4[lv];
+    const double* x = p[L.p0];
+    const double* y = p[L.p1];
+    const double* z = p[L.p2];
+    const double* w = p[L.p3];
+    int s;
+    switch (L.kind) {
+      case kO3: s = orient3d(x, y, z, w, flags); break;
+      case kO3L: s = orient3d_lifted(x, y, z, w, L.q0, L.q1, L.q2, flags); break;
+      case kO2: {
+        double v = orient2d_plain(x, y, z, L.q0, L.q1);
+        s = (v > 0.0) - (v < 0.0);
+        break;
+      }
+      case kO2L: s = orient2d_lifted(x, y, z, L.q0); break;
+      case kO1: {
+        double v = x[L.q0] - y[L.q0];
+        s = (v > 0.0) - (v < 0.0);
+        break;
+      }
+      case kO1L: s = orient1d_lifted(x, y); break;
+      default: s = 1; break;
+    }
+    if (s != 0) {
+      sg = L.flip ? -s : s;
+      break;
+    }
+  }
+  return parity ? -sg : sg;
+}
+
+// gDel3D sphere orientation with SoS: -1 = e inside the circumsphere of the
+// (orient3d_sos = +1 oriented) tet a,b,c,d; never 0.
+__device__ __forceinline__ int orient4d_sos(const double* a, const double* b, const double* c, const double* d,
+                                            const double* e, uint32_t ia, uint32_t ib, uint32_t ic, uint32_t id,
+                                            uint32_t ie, uint32_t* flags) {
+  int s = insphere(a, b, c, d, e, flags);
+  if (s != 0) return s;
+  return orient4d_sos_degenerate(a, b, c, d, e, ia, ib, ic, id, ie, flags);
+}
+
+}  // namespace ex
+}  // namespace wtet
