@@ -1,0 +1,417 @@
+"""Benchmark: exact 3D Delaunay throughput (Mpoints/s) on B200.
+
+Workload (default): one cloud of 8,000,000 float32 points, a seeded mixture of
+60% uniform in [0,1]^3, 30% Gaussian ball (centre 0.5, sigma 0.1) and 10% thin
+spherical shell (r 0.4, radial jitter 1e-4), synthetic (numpy PCG64, seed 3).
+A step = one full triangulation (normalise, sort, all insertion rounds, output
+compaction).  `--workload batched` runs 4,096 clouds of log-uniform sizes in
+[64, 65536] (uniform / Gaussian / shell / jittered lattice) as one step.
+
+  value     Mpoints/s with the points already resident in HBM (device API),
+            device-timed with CUDA events, max over ranks, whole job
+  e2e       Mpoints/s through the C ABI (wtet_delaunay_into) from pinned host
+            buffers, host->device copy of the points and device->host copy of
+            tets + adjacency inside the timed region
+  roofline  algorithmic bytes 12 B/point + 32 B/tet per triangulation over its
+            device time, against the measured HBM copy bandwidth
+  cpu_baseline  the oracle (sequential exact Bowyer-Watson restating the
+            reference's CPU path) on a bounded sample, 1 core
+
+Multi-GPU: a single cloud does not shard, so N ranks run N replicas (weak
+scaling); the batched workload splits its clouds across ranks.
+`--impl reference` times the reference's CPU algorithm (the oracle port; the
+Rust/wgpu reference cannot be built or run on this machine) with all host
+cores on the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "Mpoints/s on 1 B200 (exact 3D Delaunay, bit-identical tet set)"
+UNIT = "Mpoints/s"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def make_workload(name: str, rank: int = 0, world: int = 1):
+    import fixtures as fx
+
+    if name == "mixture8M":
+        return [fx.mixture(8_000_000, 3)]
+    if name == "uniform8M":
+        return [fx.uniform(8_000_000, 1)]
+    if name == "batched":
+        clouds = fx.batched_clouds(4096, 4)
+        return clouds[rank::world]
+    raise SystemExit(f"unknown workload {name}")
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return rank, local, world
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def run_gpu(args):
+    import torch
+
+    import wtet_b200 as wt
+
+    rank, local, world = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    wt._core.load()
+    L = wt._core.load()
+    clouds = make_workload(args.workload, rank, world)
+    n_points = sum(len(c) for c in clouds)
+    cfg = wt.Config(vote=args.vote)._c()
+
+    # ---- device-resident arm: points in HBM, output buffers preallocated ----
+    stream = torch.cuda.current_stream()
+    if len(clouds) == 1:
+        d_pts = torch.from_numpy(clouds[0]).cuda()
+        cap = int(L.wtet_max_tets(n_points))
+        d_t = torch.empty((cap, 4), dtype=torch.int32, device="cuda")
+        d_a = torch.empty((cap, 4), dtype=torch.int32, device="cuda")
+        m = ctypes.c_uint64(0)
+        st = wt._core.Stats()
+
+        def step():
+            rc = L.wtet_delaunay_device(ctypes.c_void_p(d_pts.data_ptr()), n_points, ctypes.byref(cfg),
+                                        ctypes.c_void_p(d_t.data_ptr()), ctypes.c_void_p(d_a.data_ptr()), cap,
+                                        ctypes.byref(m), ctypes.byref(st), ctypes.c_void_p(stream.cuda_stream))
+            if rc != 0:
+                raise RuntimeError(L.wtet_last_error().decode())
+            return m.value, st
+    else:
+        pts = np.ascontiguousarray(np.concatenate(clouds))
+        offsets = np.zeros(len(clouds) + 1, np.uint64)
+        offsets[1:] = np.cumsum([len(c) for c in clouds])
+        cap = int(sum(int(L.wtet_max_tets(len(c))) for c in clouds))
+        h_t = torch.empty((cap, 4), dtype=torch.int32, pin_memory=True)
+        h_a = torch.empty((cap, 4), dtype=torch.int32, pin_memory=True)
+        toff = np.zeros(len(clouds) + 1, np.uint64)
+        st = wt._core.Stats()
+        h_pts = torch.from_numpy(pts).pin_memory()
+
+        def step():
+            rc = L.wtet_delaunay_batched(ctypes.c_void_p(h_pts.data_ptr()), ctypes.c_void_p(offsets.ctypes.data),
+                                         len(clouds), ctypes.byref(cfg), ctypes.c_void_p(h_t.data_ptr()),
+                                         ctypes.c_void_p(h_a.data_ptr()), cap, ctypes.c_void_p(toff.ctypes.data),
+                                         ctypes.byref(st))
+            if rc != 0:
+                raise RuntimeError(L.wtet_last_error().decode())
+            return int(toff[-1]), st
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    dev_ms, launches, rounds, num_tets = [], 0, 0, 0
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            num_tets, s = step()
+            dev_ms.append(s.device_ms)
+            launches += s.kernel_launches
+            rounds = s.rounds
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    elapsed_ms = max_over_ranks(ev0.elapsed_time(ev1), world)
+    ms_step = elapsed_ms / args.steps
+    total_points = n_points * (world if len(clouds) == 1 else 1)
+    if len(clouds) > 1 and world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([n_points], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t)
+        total_points = int(t.item())
+    value = total_points / (ms_step * 1e3)
+
+    # ---- end-to-end arm: C ABI from pinned host buffers, copies inside ----
+    e2e = None
+    if len(clouds) == 1:
+        h_pts = torch.from_numpy(clouds[0]).pin_memory()
+        h_t = torch.empty((cap, 4), dtype=torch.int32, pin_memory=True)
+        h_a = torch.empty((cap, 4), dtype=torch.int32, pin_memory=True)
+        failed = np.empty(n_points, np.uint32)
+        st2 = wt._core.Stats()
+        m2 = ctypes.c_uint64(0)
+
+        def step_e2e():
+            rc = L.wtet_delaunay_into(ctypes.c_void_p(h_pts.data_ptr()), n_points, ctypes.byref(cfg),
+                                      ctypes.c_void_p(h_t.data_ptr()), ctypes.c_void_p(h_a.data_ptr()), cap,
+                                      ctypes.byref(m2), ctypes.c_void_p(failed.ctypes.data), ctypes.byref(st2))
+            if rc != 0:
+                raise RuntimeError(L.wtet_last_error().decode())
+
+        step_e2e()
+        torch.cuda.synchronize()
+        barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(max(1, args.steps)):
+            step_e2e()
+        torch.cuda.synchronize()
+        e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / max(1, args.steps), world)
+        e2e = {"value": round(total_points / (e2e_ms * 1e3), 4), "unit": UNIT,
+               "h2d_bytes_per_step": int(12 * n_points), "d2h_bytes_per_step": int(32 * m2.value),
+               "ms_per_step": round(e2e_ms, 3)}
+    else:
+        e2e = {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": int(12 * n_points),
+               "d2h_bytes_per_step": int(32 * num_tets), "ms_per_step": round(ms_step, 3),
+               "note": "the batched step already runs through the C ABI from pinned host buffers"}
+
+    hbm, peak_kind = peaks()
+    per_run_ms = float(np.mean(dev_ms))
+    alg_bytes = 12 * n_points + 32 * num_tets
+    achieved = alg_bytes / (per_run_ms * 1e-3) / 1e9
+    result = {
+        "metric": METRIC,
+        "value": round(value, 4),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_step, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {
+            "workload": args.workload,
+            "description": WORKLOADS[args.workload],
+            "points_per_rank": n_points,
+            "clouds_per_rank": len(clouds),
+            "vote": args.vote,
+            "parallelism": "replicas" if len(clouds) == 1 else "clouds split across ranks",
+            "l2": "working set (tets, adjacency, claims: several GB) larger than the 126 MB L2",
+        },
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "rounds": int(rounds),
+        "num_tets": int(num_tets),
+        "roofline": {
+            "bound": "hbm",
+            "achieved": round(achieved, 2),
+            "peak": hbm,
+            "unit": "GB/s",
+            "frac": round(achieved / hbm, 5),
+            "traffic": TRAFFIC.get(args.workload),
+            "basis": "whole triangulation per step: 12 B/point read + 32 B/tet written over its device time; "
+                     f"peak = {peak_kind} copy bandwidth",
+        },
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline and len(clouds) == 1:
+        result["cpu_baseline"] = cpu_baseline(clouds[0], args.cpu_sample)
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+# DRAM bytes (read + write) per triangulation measured with ncu on a 1M-point
+# case of the same distribution and scaled by the point count (profiles/).
+TRAFFIC: dict = {}
+
+WORKLOADS = {
+    "mixture8M": "8,000,000 points: 60% uniform [0,1]^3, 30% Gaussian ball (0.5, sigma 0.1), "
+                 "10% thin shell r=0.4 (jitter 1e-4); float32, seed 3",
+    "uniform8M": "8,000,000 points uniform in [0,1]^3, float32, seed 1",
+    "batched": "4,096 clouds, sizes log-uniform in [64, 65536], each uniform / Gaussian / shell / "
+               "jittered lattice, float32, seed 4",
+}
+
+
+def cpu_baseline(points, sample: int):
+    """The oracle (sequential exact Bowyer-Watson) on the first `sample` points."""
+    import oracle
+
+    sub = np.ascontiguousarray(points[:sample])
+    t0 = time.perf_counter()
+    oracle.delaunay(sub, 1)
+    dt = time.perf_counter() - t0
+    return {"value": round(len(sub) / dt / 1e6, 4), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"first {len(sub)} points of the same workload, one oracle triangulation ({dt:.1f} s)",
+            "host_cpu": host_cpu()}
+
+
+def host_cpu():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip() + f" x{os.cpu_count()}"
+    except Exception:
+        pass
+    return f"{os.cpu_count()} cpus"
+
+
+def run_reference(args):
+    """CPU reference arm: the oracle port on all host cores (independent
+    samples of the workload triangulated concurrently)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import concurrent.futures as cf
+
+    import oracle
+
+    oracle.build()
+    clouds = make_workload(args.workload)
+    threads = max(1, os.cpu_count() or 1)
+    if len(clouds) == 1:
+        pts = clouds[0]
+        chunk = min(args.cpu_sample, len(pts) // threads) if threads > 1 else args.cpu_sample
+        samples = [np.ascontiguousarray(pts[i * chunk:(i + 1) * chunk]) for i in range(threads)]
+    else:
+        samples = clouds[: threads * 4]
+    npts = sum(len(s) for s in samples)
+
+    def one_step():
+        with cf.ThreadPoolExecutor(threads) as ex:
+            list(ex.map(lambda p: oracle.delaunay(p, 1), samples))
+
+    for _ in range(args.warmup if args.warmup < 2 else 1):
+        one_step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        one_step()
+    ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    v = npts / (ms * 1e3)
+    desc = f"{len(samples)} independent samples of {npts // len(samples)} points on {threads} threads"
+    out = {"impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": args.workload, "description": WORKLOADS[args.workload]},
+           "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": threads, "kind": "port", "sample": desc,
+                            "host_cpu": host_cpu()},
+           "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "note": "reference CPU algorithm restated (oracle/); the Rust+wgpu reference cannot be built or run here"}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="wtet_b200", choices=["wtet_b200", "reference"])
+    ap.add_argument("--workload", default="mixture8M", choices=sorted(WORKLOADS))
+    ap.add_argument("--vote", default="plain", choices=["plain", "learned"])
+    ap.add_argument("--cpu-sample", type=int, default=1_000_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -76,6 +76,8 @@ typedef struct wtet_stats {
   uint64_t tets_created;      /* tets written over the whole run */
   uint64_t num_tets;          /* output tets (incl. super and infinity tets) */
   uint64_t walk_steps;        /* point-location steps */
+  uint64_t num_failed;        /* points left out as exact duplicates */
+  uint64_t kernel_launches;   /* CUDA kernels executed by the call (graph nodes included) */
   double device_ms;           /* device time of the call, CUDA events */
 } wtet_stats;
 
@@ -99,9 +101,13 @@ int wtet_delaunay(const float* xyz, uint64_t n, const wtet_config* cfg, wtet_res
 /* Same, into caller-owned host buffers of `capacity` tets each (tets and
  * adjacency, capacity x 4 u32).  *num_tets receives the count; returns
  * WTET_ERR_CAPACITY (with *num_tets set) when capacity is too small.  Pinned
- * buffers make the copies asynchronous-capable and fast. */
+ * buffers make the copies fast.  failed_verts (optional, room for n) receives
+ * the input indices left out as exact duplicates of an earlier point, count in
+ * stats->num_failed (the reference leaves duplicate handling undefined,
+ * src/tests.rs:1769-1781). */
 int wtet_delaunay_into(const float* xyz, uint64_t n, const wtet_config* cfg, uint32_t* tets,
-                       uint32_t* adjacency, uint64_t capacity, uint64_t* num_tets, wtet_stats* stats);
+                       uint32_t* adjacency, uint64_t capacity, uint64_t* num_tets, uint32_t* failed_verts,
+                       wtet_stats* stats);
 
 /* Device-resident variant (zero-copy for torch / cupy buffers): d_xyz, d_tets
  * and d_adjacency are device pointers on the current device; the work runs on

@@ -97,6 +97,9 @@ def lib():
         L.oracle_dt_num_tets.argtypes = [P]
         L.oracle_dt_copy.argtypes = [P, P, P]
         L.oracle_dt_free.argtypes = [P]
+        L.oracle_dt_num_failed.restype = ctypes.c_uint64
+        L.oracle_dt_num_failed.argtypes = [P]
+        L.oracle_dt_copy_failed.argtypes = [P, P]
         L.oracle_last_error.restype = ctypes.c_char_p
         for name in ("oracle_check_delaunay_quality", "oracle_check_local_delaunay"):
             f = getattr(L, name)
@@ -194,7 +197,9 @@ def delaunay(points, order_mode: int = 1):
     """Oracle triangulation: (tets (M,4) u32, adjacency (M,4) u32, stats dict).
 
     Vertex ids are original indices, super vertices n..n+3; adjacency is
-    (tet << 5) | face with INVALID on the super tetrahedron's hull."""
+    (tet << 5) | face with INVALID on the super tetrahedron's hull.  Exact
+    duplicates (equal normalised coordinates) after the first occurrence are
+    left out and listed in stats["failed"]."""
     pts = _f32(points)
     st = OracleStats()
     h = lib().oracle_dt_run(_ptr(pts), pts.shape[0], order_mode, ctypes.byref(st))
@@ -205,9 +210,14 @@ def delaunay(points, order_mode: int = 1):
         tets = np.empty((m, 4), np.uint32)
         adj = np.empty((m, 4), np.uint32)
         lib().oracle_dt_copy(h, _ptr(tets), _ptr(adj))
+        nf = lib().oracle_dt_num_failed(h)
+        failed = np.empty(nf, np.uint32)
+        lib().oracle_dt_copy_failed(h, _ptr(failed))
     finally:
         lib().oracle_dt_free(h)
-    return tets, adj, st.as_dict()
+    d = st.as_dict()
+    d["failed"] = failed
+    return tets, adj, d
 
 
 def check_delaunay_quality(points, tets, adj) -> int:

@@ -193,7 +193,7 @@ void build_points(const float* norm, uint32_t n, std::vector<double>& P) {
 }
 
 struct DTHandle {
-  std::vector<uint32_t> tets, adj;
+  std::vector<uint32_t> tets, adj, failed;
 };
 
 }  // namespace
@@ -325,13 +325,31 @@ void* oracle_dt_run(const float* xyz, uint64_t n64, int order_mode, oracle_stats
   } else {
     std::iota(order.begin(), order.end(), 0u);
   }
+  // Exact duplicates of the normalised coordinates: the lowest index is
+  // triangulated, later copies are reported as failed vertices.
+  std::vector<char> dup(n, 0);
+  {
+    std::vector<uint32_t> idx(n);
+    std::iota(idx.begin(), idx.end(), 0u);
+    auto key = [&](uint32_t i) {
+      uint32_t b[3];
+      std::memcpy(b, &norm[3 * size_t(i)], 12);
+      return std::array<uint32_t, 3>{b[0], b[1], b[2]};
+    };
+    std::stable_sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) { return key(a) < key(b); });
+    for (uint32_t k = 1; k < n; ++k)
+      if (key(idx[k]) == key(idx[k - 1])) dup[idx[k]] = 1;  // stable: earlier index kept
+  }
   uint32_t t = 0;
   for (uint32_t i = 0; i < n; ++i) {
     uint32_t p = order[i];
+    if (dup[p]) continue;
     if (!m.locate(p, t)) return nullptr;
     if (!m.insert(p, t)) return nullptr;
   }
   auto* h = new DTHandle;
+  for (uint32_t i = 0; i < n; ++i)
+    if (dup[i]) h->failed.push_back(i);
   std::vector<uint32_t> remap(m.V.size(), NONE);
   uint32_t cnt = 0;
   for (size_t i = 0; i < m.V.size(); ++i)
@@ -360,6 +378,11 @@ void* oracle_dt_run(const float* xyz, uint64_t n64, int order_mode, oracle_stats
 }
 
 uint64_t oracle_dt_num_tets(void* h) { return static_cast<DTHandle*>(h)->tets.size() / 4; }
+uint64_t oracle_dt_num_failed(void* h) { return static_cast<DTHandle*>(h)->failed.size(); }
+void oracle_dt_copy_failed(void* h, uint32_t* out) {
+  auto* d = static_cast<DTHandle*>(h);
+  if (out) std::memcpy(out, d->failed.data(), d->failed.size() * 4);
+}
 void oracle_dt_copy(void* h, uint32_t* tets, uint32_t* adj) {
   auto* d = static_cast<DTHandle*>(h);
   if (tets) std::memcpy(tets, d->tets.data(), d->tets.size() * 4);

@@ -62,6 +62,10 @@ uint64_t oracle_dt_num_tets(void* h);
 /* tets: (m,4) original vertex ids (super vertices n..n+3); adj: (m,4) encoded
  * (tet << 5) | face, 0xFFFFFFFF on the hull of the super tetrahedron. */
 void oracle_dt_copy(void* h, uint32_t* tets, uint32_t* adj);
+/* Input indices left out as exact duplicates (normalised coordinates equal to
+ * an earlier point's), ascending. */
+uint64_t oracle_dt_num_failed(void* h);
+void oracle_dt_copy_failed(void* h, uint32_t* out);
 void oracle_dt_free(void* h);
 const char* oracle_last_error(void);
 

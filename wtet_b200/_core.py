@@ -51,6 +51,8 @@ class Stats(ctypes.Structure):
         ("tets_created", ctypes.c_uint64),
         ("num_tets", ctypes.c_uint64),
         ("walk_steps", ctypes.c_uint64),
+        ("num_failed", ctypes.c_uint64),
+        ("kernel_launches", ctypes.c_uint64),
         ("device_ms", ctypes.c_double),
     ]
 
@@ -107,7 +109,7 @@ def load():
     L.wtet_config_default.restype = None
     L.wtet_delaunay.argtypes = [P, u64, ctypes.POINTER(_Config), ctypes.POINTER(_Result)]
     L.wtet_delaunay.restype = ctypes.c_int
-    L.wtet_delaunay_into.argtypes = [P, u64, ctypes.POINTER(_Config), P, P, u64, ctypes.POINTER(u64),
+    L.wtet_delaunay_into.argtypes = [P, u64, ctypes.POINTER(_Config), P, P, u64, ctypes.POINTER(u64), P,
                                      ctypes.POINTER(Stats)]
     L.wtet_delaunay_into.restype = ctypes.c_int
     L.wtet_delaunay_device.argtypes = [P, u64, ctypes.POINTER(_Config), P, P, u64, ctypes.POINTER(u64),
@@ -235,18 +237,19 @@ def delaunay(points, config: Config | None = None) -> DelaunayResult:
     adj = np.empty((cap, 4), np.uint32)
     m = ctypes.c_uint64(0)
     st = Stats()
+    failed = np.empty(n, np.uint32)
     rc = L.wtet_delaunay_into(_ptr(pts), n, ctypes.byref(cfg), _ptr(tets), _ptr(adj), cap, ctypes.byref(m),
-                              ctypes.byref(st))
+                              _ptr(failed), ctypes.byref(st))
     if rc == WTET_ERR_CAPACITY and m.value > cap:
         cap = m.value
         tets = np.empty((cap, 4), np.uint32)
         adj = np.empty((cap, 4), np.uint32)
         rc = L.wtet_delaunay_into(_ptr(pts), n, ctypes.byref(cfg), _ptr(tets), _ptr(adj), cap,
-                                  ctypes.byref(m), ctypes.byref(st))
+                                  ctypes.byref(m), _ptr(failed), ctypes.byref(st))
     if rc != WTET_OK:
         _raise(rc)
     k = m.value
-    return DelaunayResult(tets[:k].copy(), adj[:k].copy(), np.zeros(0, np.uint32), st.as_dict())
+    return DelaunayResult(tets[:k].copy(), adj[:k].copy(), failed[: st.num_failed].copy(), st.as_dict())
 
 
 def delaunay_batched(clouds, config: Config | None = None):

@@ -90,7 +90,7 @@ const char* wtet_last_error(void) { return g_last_error.c_str(); }
 const char* wtet_version(void) { return "0.1.0"; }
 
 int wtet_delaunay_into(const float* xyz, uint64_t n, const wtet_config* cfg, uint32_t* tets, uint32_t* adjacency,
-                       uint64_t capacity, uint64_t* num_tets, wtet_stats* stats) {
+                       uint64_t capacity, uint64_t* num_tets, uint32_t* failed_verts, wtet_stats* stats) {
   if (!xyz || !num_tets) return fail(WTET_ERR_ARG, "null pointer argument");
   if (n < 4) return fail(WTET_ERR_ARG, "Need at least 4 points for 3D Delaunay, got " + std::to_string(n));
   try {
@@ -103,7 +103,10 @@ int wtet_delaunay_into(const float* xyz, uint64_t n, const wtet_config* cfg, uin
     wtet::JobResult r = run_dev(d_xyz, {0, n}, c, s, &d_t, &d_a);
     uint64_t m = r.tet_offsets.back();
     *num_tets = m;
+    r.stats.num_failed = r.failed.size();
     fill_stats(stats, r.stats);
+    if (failed_verts)
+      for (size_t k = 0; k < r.failed.size(); ++k) failed_verts[k] = uint32_t(r.failed[k]);
     if (m > capacity || !tets || !adjacency)
       return fail(WTET_ERR_CAPACITY, "output capacity " + std::to_string(capacity) + " < " + std::to_string(m) + " tets");
     ck(cudaMemcpyAsync(tets, d_t, m * 16, cudaMemcpyDeviceToHost, s), "copy tets to host");
@@ -130,7 +133,7 @@ int wtet_delaunay(const float* xyz, uint64_t n, const wtet_config* cfg, wtet_res
     uint64_t m = r.tet_offsets.back();
     out->tets = static_cast<uint32_t*>(std::malloc(std::max<uint64_t>(m, 1) * 16));
     out->adjacency = static_cast<uint32_t*>(std::malloc(std::max<uint64_t>(m, 1) * 16));
-    out->failed_verts = static_cast<uint32_t*>(std::malloc(4));
+    out->failed_verts = static_cast<uint32_t*>(std::malloc(4 * (r.failed.size() + 1)));
     if (!out->tets || !out->adjacency || !out->failed_verts) {
       wtet_result_free(out);
       return fail(WTET_ERR_CAPACITY, "host allocation failed");
@@ -139,7 +142,9 @@ int wtet_delaunay(const float* xyz, uint64_t n, const wtet_config* cfg, wtet_res
     ck(cudaMemcpyAsync(out->adjacency, d_a, m * 16, cudaMemcpyDeviceToHost, s), "copy adjacency to host");
     ck(cudaStreamSynchronize(s), "synchronize");
     out->num_tets = m;
-    out->num_failed = 0;
+    out->num_failed = r.failed.size();
+    for (size_t k = 0; k < r.failed.size(); ++k) out->failed_verts[k] = uint32_t(r.failed[k]);
+    r.stats.num_failed = r.failed.size();
     out->stats = r.stats;
     return WTET_OK;
   } catch (const wtet::Error& e) {
@@ -164,6 +169,7 @@ int wtet_delaunay_device(const float* d_xyz, uint64_t n, const wtet_config* cfg,
     job.stream = s;
     wtet::JobResult r = wtet::run_job(job, d_tets, d_adjacency, (d_tets && d_adjacency) ? capacity : 0);
     *num_tets = r.tet_offsets.back();
+    r.stats.num_failed = r.failed.size();
     fill_stats(stats, r.stats);
     if (*num_tets > capacity || !d_tets || !d_adjacency)
       return fail(WTET_ERR_CAPACITY, "output capacity " + std::to_string(capacity) + " < " +
@@ -194,6 +200,7 @@ int wtet_delaunay_batched(const float* xyz, const uint64_t* offsets, uint32_t nu
     uint32_t *d_t = nullptr, *d_a = nullptr;
     wtet::JobResult r = run_dev(d_xyz, off, c, s, &d_t, &d_a);
     for (uint32_t k = 0; k <= num_clouds; ++k) tet_offsets[k] = r.tet_offsets[k];
+    r.stats.num_failed = r.failed.size();
     fill_stats(stats, r.stats);
     uint64_t m = r.tet_offsets.back();
     if (m > capacity || !tets || !adjacency)

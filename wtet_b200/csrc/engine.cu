@@ -52,8 +52,16 @@ constexpr uint32_t NONE = 0xFFFFFFFFu;
 constexpr uint32_t DEAD = 0xFFFFFFFFu;  // tv.x of a retired tet; tv.y then forwards to a live tet
 constexpr uint32_t INS_BIT = 0x80000000u;
 constexpr int SMALL_CAP = 80;           // cavity tets held per thread in the fast path
-constexpr uint32_t BIG_CAP = 1u << 16;  // cavity tets per large-cavity slot
-constexpr uint32_t BIG_SLOTS = 256;     // large cavities expanded per round
+// Cavity tiers: a thread with SMALL_CAP tets in registers / local memory, then
+// one warp with BIG_CAP tets in a global slot, then one warp with HUGE_CAP.
+constexpr uint32_t BIG_CAP = 1u << 12;
+constexpr uint32_t BIG_SLOTS = 1024;   // large cavities expanded per round
+constexpr uint32_t HUGE_CAP = 1u << 18;
+constexpr uint32_t HUGE_SLOTS = 16;
+// bigflag: tier (0 small, 1 big, 2 huge) | kPending while the tier applies
+// only from the next round (this round's partial claims carry its key).
+constexpr uint8_t kPending = 0x80;
+constexpr uint8_t kDup = 0x40;  // exact duplicate of an earlier point: never inserted
 constexpr uint32_t WALK_LIMIT = 1u << 22;
 constexpr int ROT_LIMIT = 1 << 16;
 constexpr int kMaxLevels = 15;
@@ -66,6 +74,7 @@ enum : uint32_t {
   kErrPrec = ex::kErrPrecision,  // 1 << 4
   kErrHull = 1u << 5,
   kErrGuard = 1u << 6,  // an index failed a range guard (never expected)
+  kErrBig = 1u << 7,    // a cavity outgrew the large-cavity slot
 };
 
 struct Counters {
@@ -76,6 +85,7 @@ struct Counters {
   uint32_t n_freed_next;  // tets retired this round
   uint32_t big_used;      // large-cavity slots used
   uint32_t n_inserted;    // winners this round
+  uint32_t huge_used;     // huge-cavity slots used
   uint32_t err;           // error flags
   unsigned long long walk_steps;
   unsigned long long n_expanded;
@@ -83,8 +93,34 @@ struct Counters {
   unsigned long long created;
 };
 
+// Round-loop state kept on the device, so that a round is a fixed kernel
+// sequence that can be replayed from a CUDA graph without host round trips.
+struct State {
+  uint32_t round;         // rounds executed
+  uint32_t n_active;      // uninserted points in the current list
+  uint32_t par;           // buffer parity: act[par] / freed[par] are current
+  uint32_t n_freed_prev;  // recyclable slots in freed[par]
+  uint32_t tet_top;       // first never-used tet slot
+  int32_t next_level;     // next stratum to locate (-1: none left)
+  uint32_t stratum_size;  // size of the last located stratum
+  uint32_t strata;
+  uint32_t act_level, act_total, act_base;  // stratum located this round
+  uint32_t done;          // all points inserted
+  uint32_t stop;          // 1 device error, 2 capacity exhausted, 3 no convergence
+  uint32_t max_rounds;
+  uint32_t carry_used, carry_left;
+  unsigned long long inserted;
+};
+
 // Everything a kernel needs, passed by value.
 struct Dev {
+  State* st;
+  uint32_t* act[2];
+  uint32_t* freed[2];
+  const struct CloudInfo* ci;
+  const uint64_t* lvl_off;    // (maxtop+1) x (nc+1) first index of each cloud per stratum
+  const uint32_t* lvl_total;  // points per stratum
+  uint32_t nc;
   // vertices (internal ids)
   float4* pts;
   uint32_t* sos;     // SoS key = cloud-local input index (super vertices n_c..n_c+3)
@@ -112,6 +148,7 @@ struct Dev {
   uint32_t* cand_base;
   uint8_t* st1;  // candidate owns its whole cavity
   uint8_t* st2;  // ... and no shared face with a better winner is violated
+  uint32_t* bigcand;  // points taking the large-cavity path this round
   uint32_t* pool;
   uint32_t pool_cap;
   uint32_t* big;
@@ -127,7 +164,27 @@ struct RoundArgs {
   uint32_t n_active;
   uint32_t n_freed_prev;
   uint32_t tet_top;
+  bool live;
 };
+
+// Reads this round's arguments from the device state and points the list
+// fields of D at the current buffers.
+__device__ __forceinline__ RoundArgs load_round(Dev& D) {
+  volatile State* S = D.st;
+  RoundArgs R;
+  R.live = !S->done && !S->stop;
+  R.round = S->round;
+  R.stamp = (unsigned long long)(~R.round) << 32;
+  R.n_active = R.live ? S->n_active : 0u;
+  R.n_freed_prev = S->n_freed_prev;
+  R.tet_top = S->tet_top;
+  const uint32_t par = S->par & 1u;
+  D.active = D.act[par];
+  D.active_next = D.act[par ^ 1u];
+  D.freed_prev = D.freed[par];
+  D.freed_next = D.freed[par ^ 1u];
+  return R;
+}
 
 __device__ __forceinline__ uint32_t comp(const uint4& v, int i) {
   return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));
@@ -338,9 +395,62 @@ __global__ void k_normalize(const float* xyz, const uint64_t* off, const CloudIn
   atomicAdd(&hist[b], 1u);
 }
 
+// Exact duplicates (equal normalised coordinates within a cloud): an open
+// addressing table keeps the lowest input index per coordinate triple.
+__device__ __forceinline__ uint32_t coord_hash(float4 q, uint32_t c) {
+  uint32_t h = mix32(__float_as_uint(q.x) ^ 0x9E3779B9u);
+  h = mix32(h ^ __float_as_uint(q.y));
+  h = mix32(h ^ __float_as_uint(q.z));
+  return mix32(h ^ c);
+}
+__device__ __forceinline__ bool same_point(float4 a, float4 b) {
+  return __float_as_uint(a.x) == __float_as_uint(b.x) && __float_as_uint(a.y) == __float_as_uint(b.y) &&
+         __float_as_uint(a.z) == __float_as_uint(b.z);
+}
+
+__global__ void k_dedup_insert(const uint64_t* off, uint32_t nc, uint64_t n, const float4* tmp, uint32_t* table,
+                               uint32_t mask) {
+  uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 q = tmp[i];
+  uint32_t c = cloud_of(off, nc, i);
+  uint32_t slot = coord_hash(q, c) & mask;
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    uint32_t cur = atomicCAS(&table[slot], NONE, uint32_t(i));
+    if (cur == NONE) return;
+    if (same_point(tmp[cur], q) && cloud_of(off, nc, cur) == c) {
+      atomicMin(&table[slot], uint32_t(i));
+      return;
+    }
+    slot = (slot + 1) & mask;
+  }
+}
+
+__global__ void k_dedup_mark(const uint64_t* off, uint32_t nc, uint64_t n, const float4* tmp,
+                             const uint32_t* table, uint32_t mask, uint8_t* dup, uint32_t* ndup) {
+  uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 q = tmp[i];
+  uint32_t c = cloud_of(off, nc, i);
+  uint32_t slot = coord_hash(q, c) & mask;
+  uint8_t d = 0;
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    uint32_t cur = table[slot];
+    if (cur == NONE) break;
+    if (same_point(tmp[cur], q) && cloud_of(off, nc, cur) == c) {
+      d = cur != uint32_t(i);
+      break;
+    }
+    slot = (slot + 1) & mask;
+  }
+  dup[i] = d;
+  if (d) atomicAdd(ndup, 1u);
+}
+
 // Scatters points into Morton order inside their cloud.
 __global__ void k_scatter_points(const uint64_t* off, const CloudInfo* ci, uint32_t nc, uint64_t n,
-                                 const float4* tmp, const uint32_t* bucket, uint32_t* cursor, Dev D) {
+                                 const float4* tmp, const uint32_t* bucket, uint32_t* cursor, const uint8_t* dup,
+                                 Dev D) {
   uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
   uint32_t c = cloud_of(off, nc, i);
@@ -350,7 +460,7 @@ __global__ void k_scatter_points(const uint64_t* off, const CloudInfo* ci, uint3
   D.sos[v] = uint32_t(i - ci[c].off);
   D.vcloud[v] = c;
   D.loc[v] = 0;
-  D.bigflag[v] = 0;
+  D.bigflag[v] = dup[i] ? kDup : 0;
   D.vtet[v] = NONE;
 }
 
@@ -384,8 +494,15 @@ __global__ void k_init_clouds(const CloudInfo* ci, uint32_t nc, Dev D) {
 // stride earlier on the Morton curve (a point of an earlier stratum: its tet
 // once inserted, else the tet that still contains it).  The located points are
 // appended to the uninserted list at position `base`.
-__global__ void k_activate(Dev D, const CloudInfo* ci, const uint64_t* lvl_off, uint32_t nc, uint32_t level,
-                           uint32_t total, uint32_t base) {
+__global__ void k_activate(Dev D) {
+  RoundArgs R = load_round(D);
+  if (!R.live) return;
+  volatile State* S = D.st;
+  const uint32_t total = S->act_total;
+  if (total == 0) return;
+  const uint32_t level = S->act_level, base = S->act_base, nc = D.nc;
+  const uint64_t* lvl_off = D.lvl_off + size_t(level) * (nc + 1);
+  const CloudInfo* ci = D.ci;
   uint32_t steps = 0;
   for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
     uint32_t lo = 0, hi = nc;
@@ -400,6 +517,8 @@ __global__ void k_activate(Dev D, const CloudInfo* ci, const uint64_t* lvl_off, 
     uint32_t stride = 1u << level;
     uint32_t pos = (level == C.top) ? k * stride : (2u * k + 1u) * stride;
     uint32_t p = C.vbase + pos;
+    D.active[base + idx] = p;
+    if (D.bigflag[p] & kDup) continue;  // never located, dropped by k_relocate
     uint32_t t = NONE;
     if (level < C.top) {
       uint32_t hv = p - stride;
@@ -415,7 +534,6 @@ __global__ void k_activate(Dev D, const CloudInfo* ci, const uint64_t* lvl_off, 
     load_pt(D.pts, p, pp);
     D.loc[p] = walk_to(D, t, p, pp, steps);
     D.bigflag[p] = 0;
-    D.active[base + idx] = p;
   }
   if (steps) atomicAdd(&D.ctr->walk_steps, (unsigned long long)steps);
 }
@@ -446,9 +564,12 @@ __device__ __forceinline__ float vote_score(const float4* pts, uint4 V, float4 q
   return (depth > 0.f && depth < 3.0e38f) ? depth : 0.f;
 }
 
-__global__ void k_vote(Dev D, RoundArgs R) {
+__global__ void k_vote(Dev D) {
+  const RoundArgs R = load_round(D);
+  if (!R.live) return;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < R.n_active; i += gridDim.x * blockDim.x) {
     uint32_t p = D.active[i];
+    if (D.bigflag[p] & kDup) continue;
     uint32_t t = D.loc[p];
     if (t >= D.cap) {
       atomicOr(&D.ctr->err, kErrGuard);
@@ -529,13 +650,27 @@ __device__ int grow_cavity(const Dev& D, uint32_t p, const double* pp, uint32_t 
   return int(K);
 }
 
-__global__ void __launch_bounds__(256) k_expand(Dev D, RoundArgs R) {
+__global__ void __launch_bounds__(256) k_expand(Dev D) {
+  const RoundArgs R = load_round(D);
+  if (!R.live) return;
   uint32_t cav[SMALL_CAP];
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < R.n_active; i += gridDim.x * blockDim.x) {
     uint32_t p = D.active[i];
+    const uint8_t tier = D.bigflag[p];
+    if (tier & kDup) continue;
     uint32_t t = D.loc[p];
-    if (D.bigflag[p] || t >= D.cap) continue;
+    if (t >= D.cap) continue;
     if (uint32_t(D.vote[t]) != ~p) continue;
+    if (tier) {
+      if (tier == 1) {
+        uint32_t b = atomicAdd(&D.ctr->big_used, 1u);
+        if (b < BIG_SLOTS) D.bigcand[b] = p;
+      } else if (tier == 2) {
+        uint32_t b = atomicAdd(&D.ctr->huge_used, 1u);
+        if (b < HUGE_SLOTS) D.bigcand[BIG_SLOTS + b] = p;
+      }
+      continue;
+    }
     D.st1[p] = 0;
     D.st2[p] = 0;
     unsigned long long key = make_key(R, p);
@@ -544,9 +679,7 @@ __global__ void __launch_bounds__(256) k_expand(Dev D, RoundArgs R) {
     int K = grow_cavity(D, p, pp, t, key, cav, SMALL_CAP);
     atomicAdd(&D.ctr->n_expanded, 1ull);
     if (K < 0) {
-      // Its partial claims carry this round's key, so the large path takes it
-      // from the next round on (k_relocate promotes 2 -> 1).
-      D.bigflag[p] = 2;
+      D.bigflag[p] = kPending | 1;
       continue;
     }
     if (K == 0) continue;
@@ -560,51 +693,138 @@ __global__ void __launch_bounds__(256) k_expand(Dev D, RoundArgs R) {
   }
 }
 
-// Large cavities: one thread per point, cavity list in a global slot.
-__global__ void k_expand_big(Dev D, RoundArgs R) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < R.n_active; i += gridDim.x * blockDim.x) {
-    uint32_t p = D.active[i];
-    if (D.bigflag[p] != 1) continue;
-    uint32_t t = D.loc[p];
-    if (t >= D.cap) continue;
-    if (uint32_t(D.vote[t]) != ~p) continue;
-    uint32_t slot = atomicAdd(&D.ctr->big_used, 1u);
-    if (slot >= BIG_SLOTS) continue;
-    D.st1[p] = 0;
-    D.st2[p] = 0;
-    uint32_t* cav = D.big + size_t(slot) * BIG_CAP;
-    unsigned long long key = make_key(R, p);
-    double pp[3];
-    load_pt(D.pts, p, pp);
-    int K = grow_cavity(D, p, pp, t, key, cav, BIG_CAP);
-    atomicAdd(&D.ctr->n_big, 1ull);
-    if (K <= 0) continue;
-    uint32_t ci = atomicAdd(&D.ctr->n_cand, 1u);
-    D.cand[ci] = p;
-    D.cand_off[ci] = 0x80000000u | slot;
-    D.cand_len[ci] = uint32_t(K);
-  }
+// Global cavity slot bi: BIG_SLOTS slots of BIG_CAP, then HUGE_SLOTS of HUGE_CAP.
+__device__ __forceinline__ uint32_t* big_slot(const Dev& D, uint32_t bi) {
+  return bi < BIG_SLOTS ? D.big + size_t(bi) * BIG_CAP
+                        : D.big + size_t(BIG_SLOTS) * BIG_CAP + size_t(bi - BIG_SLOTS) * HUGE_CAP;
 }
 
 __device__ __forceinline__ const uint32_t* cand_cavity(const Dev& D, uint32_t off) {
-  return (off & 0x80000000u) ? D.big + size_t(off & 0x7FFFFFFFu) * BIG_CAP : D.pool + off;
+  return (off & 0x80000000u) ? big_slot(D, off & 0x7FFFFFFFu) : D.pool + off;
+}
+
+#define WARP_LOOP(ci, count)                                                              \
+  for (uint32_t ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ci < (count);         \
+       ci += (gridDim.x * blockDim.x) >> 5)
+
+// Large cavities: one warp per point; the cavity list doubles as the BFS
+// queue and is grown 32 tets at a time.
+__global__ void k_expand_big(Dev D) {
+  const RoundArgs R = load_round(D);
+  if (!R.live) return;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t nbig = min(*(volatile uint32_t*)&D.ctr->big_used, BIG_SLOTS);
+  const uint32_t nhuge = min(*(volatile uint32_t*)&D.ctr->huge_used, HUGE_SLOTS);
+  WARP_LOOP(wi, nbig + nhuge) {
+    const bool huge = wi >= nbig;
+    const uint32_t bi = huge ? BIG_SLOTS + (wi - nbig) : wi;
+    const uint32_t cap = huge ? HUGE_CAP : BIG_CAP;
+    uint32_t p = D.bigcand[bi];
+    uint32_t t0 = D.loc[p];
+    uint32_t* cav = big_slot(D, bi);
+    unsigned long long key = make_key(R, p);
+    double pp[3];
+    load_pt(D.pts, p, pp);
+    int lost = 0;
+    if (lane == 0) {
+      D.st1[p] = 0;
+      D.st2[p] = 0;
+      unsigned long long old = atomicMin(&D.ccav[t0], key);
+      lost = old < key;
+      cav[0] = t0;
+    }
+    lost = __shfl_sync(0xFFFFFFFFu, lost, 0);
+    uint32_t K = 1, head = 0;
+    bool overflow = false;
+    __syncwarp();
+    while (!lost && !overflow && head < K) {
+      uint32_t idx = head + lane;
+      bool valid = idx < K;
+      uint32_t c = valid ? cav[idx] : 0u;
+      uint4 N = valid ? D.tn[c] : make_uint4(NONE, NONE, NONE, NONE);
+      uint32_t newK = K;
+      bool my_lost = false, my_guard = false;
+      for (int f = 0; f < 4; ++f) {
+        bool add = false;
+        uint32_t nt = 0;
+        uint32_t nb = comp(N, f);
+        if (valid && nb != NONE) {
+          nt = nb >> 2;
+          if (nt >= D.cap) {
+            my_guard = true;
+          } else if (__ldcg(&D.ccav[nt]) != key && __ldcg(&D.cring[nt]) != key) {
+            uint4 W = D.tv[nt];
+            if (W.x >= D.nv || W.y >= D.nv || W.z >= D.nv || W.w >= D.nv) {
+              my_guard = true;
+            } else {
+              double P[4][3];
+              load_pt(D.pts, W.x, P[0]);
+              load_pt(D.pts, W.y, P[1]);
+              load_pt(D.pts, W.z, P[2]);
+              load_pt(D.pts, W.w, P[3]);
+              int sg = o4d_sos(P[0], P[1], P[2], P[3], pp, W.x, W.y, W.z, W.w, p, D.sos, &D.ctr->err);
+              if (sg < 0) {
+                unsigned long long old = atomicMin(&D.ccav[nt], key);
+                if (old < key) my_lost = true;
+                else if (old != key) add = true;
+              } else {
+                D.cring[nt] = key;
+              }
+            }
+          }
+        }
+        unsigned ball = __ballot_sync(0xFFFFFFFFu, add);
+        uint32_t pos = newK + __popc(ball & ((1u << lane) - 1u));
+        if (add) {
+          if (pos < cap) cav[pos] = nt;
+          else overflow = true;
+        }
+        newK += __popc(ball);
+      }
+      if (__any_sync(0xFFFFFFFFu, my_guard)) {
+        if (lane == 0) atomicOr(&D.ctr->err, kErrGuard);
+        lost = 1;
+      }
+      lost |= __any_sync(0xFFFFFFFFu, my_lost);
+      overflow = __any_sync(0xFFFFFFFFu, overflow);
+      head = min(head + 32u, K);
+      K = newK;
+      __syncwarp();
+    }
+    if (lane == 0) atomicAdd(&D.ctr->n_big, 1ull);
+    if (overflow) {
+      if (lane == 0) {
+        if (huge) atomicOr(&D.ctr->err, kErrBig);
+        else D.bigflag[p] = kPending | 2;
+      }
+      continue;
+    }
+    if (lost) continue;
+    if (lane == 0) {
+      uint32_t ci = atomicAdd(&D.ctr->n_cand, 1u);
+      D.cand[ci] = p;
+      D.cand_off[ci] = 0x80000000u | bi;
+      D.cand_len[ci] = K;
+    }
+  }
 }
 
 // A candidate wins its cavity when it holds the minimum claim on every tet.
-__global__ void k_resolve(Dev D, RoundArgs R) {
+__global__ void k_resolve(Dev D) {
+  const RoundArgs R = load_round(D);
+  if (!R.live) return;
+  const uint32_t lane = threadIdx.x & 31;
   const uint32_t ncand = *(volatile uint32_t*)&D.ctr->n_cand;
-  for (uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x; ci < ncand; ci += gridDim.x * blockDim.x) {
+  WARP_LOOP(ci, ncand) {
     uint32_t p = D.cand[ci];
     uint32_t K = D.cand_len[ci];
     const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
     unsigned long long key = make_key(R, p);
-    bool win = true;
-    for (uint32_t i = 0; i < K; ++i)
-      if (__ldcg(&D.ccav[cav[i]]) != key) {
-        win = false;
-        break;
-      }
-    D.st1[p] = win ? 1 : 0;
+    bool ok = true;
+    for (uint32_t i = lane; i < K; i += 32)
+      if (__ldcg(&D.ccav[cav[i]]) != key) ok = false;
+    bool win = __all_sync(0xFFFFFFFFu, ok);
+    if (lane == 0) D.st1[p] = win ? 1 : 0;
   }
 }
 
@@ -612,21 +832,24 @@ __global__ void k_resolve(Dev D, RoundArgs R) {
 // Delaunay: the better winner q must lie outside the circumsphere of the
 // worse winner p's new tet on f (then either insertion order gives the same
 // tets).  The worse one of a violating pair steps back.
-__global__ void k_shared(Dev D, RoundArgs R) {
+__global__ void k_shared(Dev D) {
+  const RoundArgs R = load_round(D);
+  if (!R.live) return;
+  const uint32_t lane = threadIdx.x & 31;
   const uint32_t ncand = *(volatile uint32_t*)&D.ctr->n_cand;
-  for (uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x; ci < ncand; ci += gridDim.x * blockDim.x) {
+  WARP_LOOP(ci, ncand) {
     uint32_t p = D.cand[ci];
     if (!D.st1[p]) {
-      D.st2[p] = 0;
+      if (lane == 0) D.st2[p] = 0;
       continue;
     }
     uint32_t K = D.cand_len[ci];
     const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
     unsigned long long key = make_key(R, p);
-    bool ok = true;
+    bool bad = false;
     double pp[3];
     load_pt(D.pts, p, pp);
-    for (uint32_t i = 0; i < K && ok; ++i) {
+    for (uint32_t i = lane; i < K && !bad; i += 32) {
       uint32_t c = cav[i];
       uint4 N = D.tn[c];
       for (int f = 0; f < 4; ++f) {
@@ -647,12 +870,13 @@ __global__ void k_shared(Dev D, RoundArgs R) {
         double qq[3];
         load_pt(D.pts, q, qq);
         if (o4d_sos(P[0], P[1], P[2], P[3], qq, w[0], w[1], w[2], w[3], q, D.sos, &D.ctr->err) < 0) {
-          ok = false;
+          bad = true;
           break;
         }
       }
     }
-    D.st2[p] = ok ? 1 : 0;
+    bool viol = __any_sync(0xFFFFFFFFu, bad);
+    if (lane == 0) D.st2[p] = viol ? 0 : 1;
   }
 }
 
@@ -665,53 +889,69 @@ __device__ __forceinline__ bool boundary_face(const Dev& D, uint32_t nb, unsigne
 }
 
 // Hands out one slot per boundary face (recycled slots first, then fresh ones).
-__global__ void k_alloc(Dev D, RoundArgs R) {
+__global__ void k_alloc(Dev D) {
+  const RoundArgs R = load_round(D);
+  if (!R.live) return;
+  const uint32_t lane = threadIdx.x & 31;
   const uint32_t ncand = *(volatile uint32_t*)&D.ctr->n_cand;
-  for (uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x; ci < ncand; ci += gridDim.x * blockDim.x) {
+  WARP_LOOP(ci, ncand) {
     uint32_t p = D.cand[ci];
     if (!D.st2[p]) continue;
     uint32_t K = D.cand_len[ci];
     const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
     unsigned long long key = make_key(R, p);
-    uint32_t F = 0;
-    for (uint32_t i = 0; i < K; ++i) {
+    uint32_t Fl = 0;
+    for (uint32_t i = lane; i < K; i += 32) {
       uint4 N = D.tn[cav[i]];
-      for (int f = 0; f < 4; ++f) F += boundary_face(D, comp(N, f), key);
+      for (int f = 0; f < 4; ++f) Fl += boundary_face(D, comp(N, f), key);
     }
-    uint32_t base = atomicAdd(&D.ctr->alloc_used, F);
-    uint32_t last = base + F;
+    uint32_t incl = Fl;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= uint32_t(o)) incl += y;
+    }
+    uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&D.ctr->alloc_used, total);
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    uint32_t last = base + total;
     if (last > R.n_freed_prev && R.tet_top + (last - R.n_freed_prev) > D.cap) {
-      atomicOr(&D.ctr->err, kErrCapacity);
-      D.st2[p] = 0;
+      if (lane == 0) {
+        atomicOr(&D.ctr->err, kErrCapacity);
+        D.st2[p] = 0;
+      }
       continue;
     }
-    uint32_t j = 0;
-    for (uint32_t i = 0; i < K; ++i) {
+    uint32_t j = base + incl - Fl;
+    for (uint32_t i = lane; i < K; i += 32) {
       uint32_t c = cav[i];
       uint4 N = D.tn[c];
       uint4 S = make_uint4(NONE, NONE, NONE, NONE);
       for (int f = 0; f < 4; ++f)
-        if (boundary_face(D, comp(N, f), key)) set_comp(S, f, slot_of(D, R, base + j++));
+        if (boundary_face(D, comp(N, f), key)) set_comp(S, f, slot_of(D, R, j++));
       D.nslot[c] = S;
     }
-    D.cand_base[ci] = base;
+    if (lane == 0) D.cand_base[ci] = base;
   }
 }
 
 // Writes the new tets of every winner.  Faces through p are matched by
 // rotating around the boundary edge inside the cavity; a boundary face shared
 // with another winner's cavity links to that winner's new tet.
-__global__ void __launch_bounds__(128) k_write(Dev D, RoundArgs R) {
+__global__ void __launch_bounds__(128) k_write(Dev D) {
+  const RoundArgs R = load_round(D);
+  if (!R.live) return;
+  const uint32_t lane = threadIdx.x & 31;
   const uint32_t ncand = *(volatile uint32_t*)&D.ctr->n_cand;
-  for (uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x; ci < ncand; ci += gridDim.x * blockDim.x) {
+  WARP_LOOP(ci, ncand) {
     uint32_t p = D.cand[ci];
     if (!D.st2[p]) continue;
     uint32_t K = D.cand_len[ci];
     const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
     unsigned long long key = make_key(R, p);
-    uint32_t F = 0;
+    uint32_t Fl = 0;
     bool bad = false;
-    for (uint32_t i = 0; i < K; ++i) {
+    for (uint32_t i = lane; i < K; i += 32) {
       uint32_t c = cav[i];
       uint4 V = D.tv[c];
       uint4 N = D.tn[c];
@@ -719,7 +959,7 @@ __global__ void __launch_bounds__(128) k_write(Dev D, RoundArgs R) {
       for (int f = 0; f < 4; ++f) {
         uint32_t s = comp(S, f);
         if (s == NONE) continue;
-        ++F;
+        ++Fl;
         uint32_t outer = comp(N, f);
         bool shared = false;
         uint32_t link_out = outer;
@@ -769,39 +1009,55 @@ __global__ void __launch_bounds__(128) k_write(Dev D, RoundArgs R) {
         }
         D.tv[s] = nv;
         D.tn[s] = nn;
+        // Every vertex on the cavity boundary gets a live incident tet, so a
+        // vertex's hint tet is alive whenever it is read (strata activation).
+        for (int q = 0; q < 4; ++q)
+          if (q != f) D.vtet[comp(V, q)] = s;
         if (outer != NONE && !shared && (outer >> 2) < D.cap) {
           uint32_t* w = reinterpret_cast<uint32_t*>(&D.tn[outer >> 2]) + (outer & 3);
           *w = (s << 2) | uint32_t(f);
         }
       }
     }
-    if (bad) atomicOr(&D.ctr->err, kErrRotate);
-    // Retire the cavity, forwarding to a new tet of p.
-    uint32_t s0 = slot_of(D, R, D.cand_base[ci]);
-    for (uint32_t i = 0; i < K; ++i) {
+    if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) atomicOr(&D.ctr->err, kErrRotate);
+    __syncwarp();  // every lane is done reading the cavity before it is retired
+    const uint32_t s0 = slot_of(D, R, D.cand_base[ci]);
+    uint32_t fbase = 0;
+    if (lane == 0) fbase = atomicAdd(&D.ctr->n_freed_next, K);
+    fbase = __shfl_sync(0xFFFFFFFFu, fbase, 0);
+    for (uint32_t i = lane; i < K; i += 32) {
       uint32_t c = cav[i];
-      D.tv[c] = make_uint4(DEAD, s0, 0u, 0u);
+      // Points inside c relocate from a new tet on one of c's own faces.
+      uint4 S = D.nslot[c];
+      uint32_t fwd = S.x != NONE ? S.x : S.y != NONE ? S.y : S.z != NONE ? S.z : S.w != NONE ? S.w : s0;
+      D.tv[c] = make_uint4(DEAD, fwd, 0u, 0u);
+      D.freed_next[fbase + i] = c;
     }
-    uint32_t fbase = atomicAdd(&D.ctr->n_freed_next, K);
-    for (uint32_t i = 0; i < K; ++i) D.freed_next[fbase + i] = cav[i];
-    D.vtet[p] = s0;
-    D.loc[p] |= INS_BIT;
-    D.centry[D.vcloud[p]] = s0;
-    D.bigflag[p] = 0;
-    atomicAdd(&D.ctr->n_inserted, 1u);
-    atomicAdd(&D.ctr->created, (unsigned long long)F);
+    for (int o = 16; o > 0; o >>= 1) Fl += __shfl_xor_sync(0xFFFFFFFFu, Fl, o);
+    if (lane == 0) {
+      D.vtet[p] = s0;
+      D.loc[p] |= INS_BIT;
+      D.centry[D.vcloud[p]] = s0;
+      D.bigflag[p] = 0;
+      atomicAdd(&D.ctr->n_inserted, 1u);
+      atomicAdd(&D.ctr->created, (unsigned long long)Fl);
+    }
   }
 }
 
 // Clears the votes, relocates points whose tet was retired, and compacts the
 // uninserted list.
-__global__ void k_relocate(Dev D, RoundArgs R) {
+__global__ void k_relocate(Dev D) {
+  const RoundArgs R = load_round(D);
+  if (!R.live) return;
   uint32_t steps = 0;
   for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < R.n_active; i0 += gridDim.x * blockDim.x) {
     uint32_t i = i0 + threadIdx.x;
     bool keep = false;
     uint32_t p = 0;
-    if (i < R.n_active) {
+    if (i < R.n_active && (D.bigflag[D.active[i]] & kDup)) {
+      // exact duplicate: leaves the list without being inserted
+    } else if (i < R.n_active) {
       p = D.active[i];
       uint32_t L = D.loc[p];
       uint32_t t = L & ~INS_BIT;
@@ -813,7 +1069,7 @@ __global__ void k_relocate(Dev D, RoundArgs R) {
       D.vote[t] = 0ull;
       if (!(L & INS_BIT)) {
         keep = true;
-        if (D.bigflag[p] == 2) D.bigflag[p] = 1;
+        if (D.bigflag[p] & kPending) D.bigflag[p] &= uint8_t(~kPending);
         uint4 V = D.tv[t];
         if (V.x == DEAD) {
           double pp[3];
@@ -826,6 +1082,78 @@ __global__ void k_relocate(Dev D, RoundArgs R) {
     if (keep) D.active_next[slot] = p;
   }
   if (steps) atomicAdd(&D.ctr->walk_steps, (unsigned long long)steps);
+}
+
+// Start of a round: locate the next stratum once the current one has thinned
+// to a quarter, stop when nothing is left, reset the per-round counters.
+__global__ void k_begin(Dev D) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  State* S = D.st;
+  if (S->done || S->stop) return;
+  S->act_total = 0;
+  while (S->next_level >= 0 && (S->n_active == 0 || 4ull * S->n_active <= S->stratum_size)) {
+    const int L = S->next_level--;
+    const uint32_t total = D.lvl_total[L];
+    if (total == 0) continue;
+    S->act_level = uint32_t(L);
+    S->act_total = total;
+    S->act_base = S->n_active;
+    S->n_active += total;
+    S->stratum_size = total;
+    S->strata += 1;
+    break;
+  }
+  if (S->n_active == 0) {
+    S->done = 1;
+    return;
+  }
+  S->round += 1;
+  if (S->round > S->max_rounds) {
+    S->stop = 3;
+    return;
+  }
+  Counters* C = D.ctr;
+  C->n_next = 0;
+  C->n_cand = 0;
+  C->pool_used = 0;
+  C->alloc_used = 0;
+  C->n_freed_next = 0;
+  C->big_used = 0;
+  C->n_inserted = 0;
+  C->huge_used = 0;
+}
+
+// Recycled slots that were not handed out this round carry over.
+__global__ void k_carry(Dev D) {
+  const RoundArgs R = load_round(D);
+  if (!R.live) return;
+  const uint32_t used = *(volatile uint32_t*)&D.ctr->alloc_used;
+  const uint32_t nfn = *(volatile uint32_t*)&D.ctr->n_freed_next;
+  if (R.n_freed_prev <= used) return;
+  const uint32_t left = R.n_freed_prev - used;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < left; i += gridDim.x * blockDim.x)
+    D.freed_next[nfn + i] = D.freed_prev[used + i];
+}
+
+// End of a round: advance the slot top, swap the lists, stop on errors.
+__global__ void k_end(Dev D) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  State* S = D.st;
+  if (S->done || S->stop) return;
+  Counters* C = D.ctr;
+  if (C->err & ~uint32_t(kErrCapacity)) {
+    S->stop = 1;
+    return;
+  }
+  const uint32_t used = C->alloc_used;
+  const uint32_t fresh = used > S->n_freed_prev ? used - S->n_freed_prev : 0u;
+  const uint32_t left = S->n_freed_prev > used ? S->n_freed_prev - used : 0u;
+  S->tet_top += fresh;
+  S->n_freed_prev = C->n_freed_next + left;
+  S->par ^= 1u;
+  S->n_active = C->n_next;
+  S->inserted += C->n_inserted;
+  if (C->err & kErrCapacity) S->stop = 2;
 }
 
 // --------------------------------------------------------------- output ----
@@ -1039,17 +1367,20 @@ struct DBuf {
 };
 
 // Exclusive scan in place over n u32 (recursive over block sums).
-void scan_u32(uint32_t* d, uint32_t n, cudaStream_t s, std::vector<DBuf<uint32_t>>& tmp, int depth = 0) {
-  if (n == 0) return;
+int scan_u32(uint32_t* d, uint32_t n, cudaStream_t s, std::vector<DBuf<uint32_t>>& tmp, int depth = 0) {
+  if (n == 0) return 0;
   const uint32_t threads = 256, per_block = threads * 4;
   uint32_t blocks = (n + per_block - 1) / per_block;
   if (int(tmp.size()) <= depth) tmp.resize(depth + 1);
   tmp[depth].reserve(size_t(blocks) + 1, "scan sums");
   k_scan_blocks<<<blocks, threads, 0, s>>>(d, d, tmp[depth].p, n);
+  int launches = 1;
   if (blocks > 1) {
-    scan_u32(tmp[depth].p, blocks, s, tmp, depth + 1);
+    launches += scan_u32(tmp[depth].p, blocks, s, tmp, depth + 1);
     k_scan_add<<<blocks, threads, 0, s>>>(d, tmp[depth].p, n);
+    ++launches;
   }
+  return launches;
 }
 
 uint32_t initial_stride_log2(uint64_t n) {
@@ -1083,15 +1414,20 @@ struct Workspace {
   DBuf<unsigned long long> ccav, cring, vote;
   DBuf<uint32_t> centry, active, active_next, cand, cand_off, cand_len, cand_base, pool, big, freed_a, freed_b;
   DBuf<uint8_t> st1, st2;
+  DBuf<uint32_t> bigcand;
   DBuf<uint64_t> lvl_off;
+  DBuf<uint32_t> lvl_total;
+  DBuf<State> state;
   DBuf<Counters> ctr;
   DBuf<uint32_t> ccount, hullcnt, cfill, newid;
   DBuf<uint2> hull;
   DBuf<uint64_t> coff;
-  DBuf<uint32_t> out_t, out_a;
+  DBuf<uint32_t> out_t, out_a, dtab;
+  DBuf<uint8_t> dup;
   std::vector<DBuf<uint32_t>> scan_tmp;
   Counters* h_ctr = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaStream_t stream = nullptr;
   int device = -1;
 
   ~Workspace() {
@@ -1115,6 +1451,7 @@ Workspace& ws() {
     ck(cudaEventCreate(&tl_ws->ev0), "event");
     ck(cudaEventCreate(&tl_ws->ev1), "event");
   }
+  if (!tl_ws->stream) ck(cudaStreamCreate(&tl_ws->stream), "stream");
   return *tl_ws;
 }
 
@@ -1150,14 +1487,15 @@ void release_thread_workspace() {
   w.vcloud.release(); w.vtet.release(); w.loc.release(); w.bigflag.release(); w.tv.release();
   w.tn.release(); w.nslot.release(); w.ccav.release(); w.cring.release(); w.vote.release();
   w.centry.release(); w.active.release(); w.active_next.release(); w.cand.release();
-  w.cand_off.release(); w.cand_len.release(); w.cand_base.release(); w.st1.release(); w.st2.release(); w.pool.release(); w.big.release();
-  w.freed_a.release(); w.freed_b.release(); w.lvl_off.release(); w.ctr.release();
+  w.cand_off.release(); w.cand_len.release(); w.cand_base.release(); w.st1.release(); w.st2.release(); w.bigcand.release(); w.pool.release(); w.big.release();
+  w.freed_a.release(); w.freed_b.release(); w.lvl_off.release(); w.lvl_total.release(); w.state.release(); w.ctr.release();
   w.ccount.release(); w.hullcnt.release(); w.cfill.release(); w.newid.release();
-  w.hull.release(); w.coff.release(); w.out_t.release(); w.out_a.release();
+  w.hull.release(); w.coff.release(); w.out_t.release(); w.out_a.release(); w.dtab.release(); w.dup.release();
   for (auto& b : w.scan_tmp) b.release();
   if (w.h_ctr) cudaFreeHost(w.h_ctr);
   if (w.ev0) cudaEventDestroy(w.ev0);
   if (w.ev1) cudaEventDestroy(w.ev1);
+  if (w.stream) cudaStreamDestroy(w.stream);
   delete tl_ws;
   tl_ws = nullptr;
 }
@@ -1189,7 +1527,9 @@ void reserve_stack_once() {
 JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t capacity) {
   reserve_stack_once();
   Workspace& W = ws();
-  cudaStream_t s = job.stream;
+  // The legacy default stream cannot be captured into a graph; the workspace's
+  // own (blocking) stream orders with it implicitly.
+  cudaStream_t s = job.stream ? job.stream : W.stream;
   const uint32_t nc = uint32_t(job.offsets.size() - 1);
   const uint64_t n = job.offsets.back();
   if (n + 5ull * nc >= 0x7FFFFFF0ull) throw Error{WTET_ERR_ARG, "too many points for 31-bit vertex ids"};
@@ -1241,12 +1581,15 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   W.cand_len.reserve(n, "cand");
   W.cand_base.reserve(n, "cand");
   W.st1.reserve(nv, "status");
+  W.bigcand.reserve(BIG_SLOTS + HUGE_SLOTS, "bigcand");
   W.st2.reserve(nv, "status");
   const uint32_t pool_cap = uint32_t(std::min<uint64_t>(std::max<uint64_t>(n * 24, 1 << 16), 1ull << 30));
   W.pool.reserve(pool_cap, "pool");
-  W.big.reserve(size_t(BIG_SLOTS) * BIG_CAP, "big");
+  W.big.reserve(size_t(BIG_SLOTS) * BIG_CAP + size_t(HUGE_SLOTS) * HUGE_CAP, "big");
   W.ctr.reserve(1, "counters");
   W.lvl_off.reserve(size_t(maxtop + 1) * (nc + 1), "levels");
+  W.lvl_total.reserve(maxtop + 1, "levels");
+  W.state.reserve(1, "state");
   W.ccount.reserve(nc, "ccount");
   W.hullcnt.reserve(nc, "hull");
   W.cfill.reserve(nc, "cfill");
@@ -1283,8 +1626,11 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     D.bigflag = W.bigflag.p; D.tv = W.tv.p; D.tn = W.tn.p; D.ccav = W.ccav.p; D.cring = W.cring.p;
     D.nslot = W.nslot.p; D.vote = W.vote.p; D.cap = uint32_t(cap); D.nv = uint32_t(nv); D.centry = W.centry.p;
     D.active = W.active.p; D.active_next = W.active_next.p; D.cand = W.cand.p; D.cand_off = W.cand_off.p;
-    D.cand_len = W.cand_len.p; D.cand_base = W.cand_base.p; D.st1 = W.st1.p; D.st2 = W.st2.p; D.pool = W.pool.p; D.pool_cap = pool_cap; D.big = W.big.p;
+    D.cand_len = W.cand_len.p; D.cand_base = W.cand_base.p; D.st1 = W.st1.p; D.st2 = W.st2.p; D.bigcand = W.bigcand.p; D.pool = W.pool.p; D.pool_cap = pool_cap; D.big = W.big.p;
     D.freed_prev = W.freed_a.p; D.freed_next = W.freed_b.p; D.ctr = W.ctr.p;
+    D.st = W.state.p; D.act[0] = W.active.p; D.act[1] = W.active_next.p;
+    D.freed[0] = W.freed_a.p; D.freed[1] = W.freed_b.p; D.ci = W.ci.p; D.lvl_off = W.lvl_off.p;
+    D.lvl_total = W.lvl_total.p; D.nc = nc;
     D.rule = int(job.cfg.insertion_rule == WTET_RULE_CENTROID ? 1 : 0);
   };
   refresh();
@@ -1294,10 +1640,28 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   uint32_t nb = uint32_t((n + T - 1) / T);
   k_bbox<<<nb, T, 0, s>>>(job.d_xyz, W.off.p, nc, n, W.mn.p, W.mx.p);
   k_normalize<<<nb, T, 0, s>>>(job.d_xyz, W.off.p, W.ci.p, nc, n, W.mn.p, W.mx.p, W.tmp.p, W.bucket.p, W.hist.p);
-  scan_u32(W.hist.p, uint32_t(buckets + 1), s, W.scan_tmp);
-  k_scatter_points<<<nb, T, 0, s>>>(W.off.p, W.ci.p, nc, n, W.tmp.p, W.bucket.p, W.hist.p, D);
+  uint32_t hmask = 1;
+  while (hmask < 2 * n) hmask <<= 1;
+  W.dtab.reserve(hmask, "dedup table");
+  W.dup.reserve(n, "dedup flags");
+  hmask -= 1;
+  ck(cudaMemsetAsync(W.dtab.p, 0xFF, size_t(hmask + 1) * 4, s), "memset");
+  k_dedup_insert<<<nb, T, 0, s>>>(W.off.p, nc, n, W.tmp.p, W.dtab.p, hmask);
+  k_dedup_mark<<<nb, T, 0, s>>>(W.off.p, nc, n, W.tmp.p, W.dtab.p, hmask, W.dup.p, &W.ctr.p->huge_used);
+  uint64_t launches = 7;  // bbox, normalize, dedup x2, scatter, init, plus the scan below
+  launches += scan_u32(W.hist.p, uint32_t(buckets + 1), s, W.scan_tmp);
+  k_scatter_points<<<nb, T, 0, s>>>(W.off.p, W.ci.p, nc, n, W.tmp.p, W.bucket.p, W.hist.p, W.dup.p, D);
   k_init_clouds<<<(nc + 127) / 128, 128, 0, s>>>(W.ci.p, nc, D);
   ck(cudaGetLastError(), "setup kernels");
+  uint32_t ndup = 0;
+  ck(cudaMemcpyAsync(&ndup, &W.ctr.p->huge_used, 4, cudaMemcpyDeviceToHost, s), "d2h");
+  ck(cudaStreamSynchronize(s), "dedup");
+  if (ndup) {
+    std::vector<uint8_t> flags(n);
+    ck(cudaMemcpy(flags.data(), W.dup.p, n, cudaMemcpyDeviceToHost), "d2h");
+    for (uint64_t i = 0; i < n; ++i)
+      if (flags[i]) res.failed.push_back(i);
+  }
 
   // ---- strata table: lvl_off[L][c] = first index of cloud c in stratum L ----
   std::vector<uint64_t> lvl(size_t(maxtop + 1) * (nc + 1));
@@ -1313,9 +1677,6 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   }
   ck(cudaMemcpyAsync(W.lvl_off.p, lvl.data(), lvl.size() * 8, cudaMemcpyHostToDevice, s), "h2d");
 
-  uint32_t tet_top = nc;
-  uint32_t n_freed_prev = 0;
-  uint32_t round = 0;
   wtet_stats st{};
   // max_insert_iterations bounds the rounds of each stratum (src/types.rs:44-46).
   const uint32_t max_rounds = std::max<uint32_t>(job.cfg.max_insert_iterations, 1u) * (maxtop + 1);
@@ -1326,127 +1687,106 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     for (auto& e : tev) cudaEventCreate(&e);
   const uint32_t TB = 256;
 
-  int next_level = int(maxtop);
-  uint32_t n_active = 0, stratum_size = 0;
+  // ---- the round loop, driven from device state and replayed from a graph ----
+  std::vector<uint32_t> lt(maxtop + 1);
+  for (uint32_t L = 0; L <= maxtop; ++L) lt[L] = lvl_total[L];
+  ck(cudaMemcpyAsync(W.lvl_total.p, lt.data(), (maxtop + 1) * 4, cudaMemcpyHostToDevice, s), "h2d");
+  State S0{};
+  S0.tet_top = nc;
+  S0.next_level = int32_t(maxtop);
+  S0.max_rounds = max_rounds;
+  ck(cudaMemcpyAsync(W.state.p, &S0, sizeof(State), cudaMemcpyHostToDevice, s), "h2d");
   ck(cudaMemsetAsync(W.ctr.p, 0, sizeof(Counters), s), "memset");
+
+  const uint32_t GT = 148 * 8;         // thread kernels: 256-thread blocks, grid-stride
+  const uint32_t GW = 148 * 16;        // warp-per-candidate kernels: 128-thread blocks
+  const uint32_t GB = (BIG_SLOTS + HUGE_SLOTS) / 4;
+  auto enqueue_round = [&]() {
+    k_begin<<<1, 32, 0, s>>>(D);
+    k_activate<<<GT, TB, 0, s>>>(D);
+    k_vote<<<GT, TB, 0, s>>>(D);
+    k_expand<<<GT, TB, 0, s>>>(D);
+    k_expand_big<<<GB, 128, 0, s>>>(D);
+    k_resolve<<<GW, 128, 0, s>>>(D);
+    k_shared<<<GW, 128, 0, s>>>(D);
+    k_alloc<<<GW, 128, 0, s>>>(D);
+    k_write<<<GW, 128, 0, s>>>(D);
+    k_relocate<<<GT, TB, 0, s>>>(D);
+    k_carry<<<148, TB, 0, s>>>(D);
+    k_end<<<1, 32, 0, s>>>(D);
+  };
+  // Rounds per host check (the graph holds this many rounds).
+  uint32_t rpg = job.rounds_per_graph ? job.rounds_per_graph : 8u;
+  if (trace) rpg = 1;
+  cudaGraphExec_t gexec = nullptr;
+  auto build_graph = [&]() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    gexec = nullptr;
+    cudaGraph_t g = nullptr;
+    ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+    for (uint32_t r = 0; r < rpg; ++r) enqueue_round();
+    ck(cudaStreamEndCapture(s, &g), "end capture");
+    ck(cudaGraphInstantiate(&gexec, g, 0), "graph instantiate");
+    cudaGraphDestroy(g);
+  };
+  build_graph();
+  State hs{};
   for (;;) {
-    // Strata overlap: the next one is located once the uninserted points of
-    // the current one have thinned to a quarter, which keeps rounds full.
-    while (next_level >= 0 && (n_active == 0 || 4ull * n_active <= stratum_size)) {
-      const int L = next_level--;
-      const uint32_t total = lvl_total[L];
-      if (total == 0) continue;
-      k_activate<<<blocks_for(total, TB), TB, 0, s>>>(D, W.ci.p, W.lvl_off.p + size_t(L) * (nc + 1), nc,
-                                                      uint32_t(L), total, n_active);
-      n_active += total;
-      stratum_size = total;
-      ++st.strata;
-      break;
-    }
-    if (n_active == 0) break;
-    ++round;
-    if (round > max_rounds) throw Error{WTET_ERR_NO_CONVERGE, "insertion did not converge within max_insert_iterations"};
-    RoundArgs R;
-    R.stamp = (unsigned long long)(~round) << 32;
-    R.round = round;
-    R.n_active = n_active;
-    R.n_freed_prev = n_freed_prev;
-    R.tet_top = tet_top;
-    // Reset the per-round counters; walk / statistics counters accumulate.
-    ck(cudaMemsetAsync(W.ctr.p, 0, offsetof(Counters, err), s), "memset");
-    const uint32_t g = blocks_for(n_active, TB);
-    const uint32_t gc = blocks_for(n_active, 128);
-    auto mark = [&](int i) {
-      if (trace >= 3) cudaEventRecord(tev[i], s);
-    };
-    mark(0);
-    k_vote<<<g, TB, 0, s>>>(D, R);
-    mark(1);
-    k_expand<<<g, TB, 0, s>>>(D, R);
-    mark(2);
-    k_expand_big<<<g, TB, 0, s>>>(D, R);
-    mark(3);
-    k_resolve<<<gc, 128, 0, s>>>(D, R);
-    mark(4);
-    k_shared<<<gc, 128, 0, s>>>(D, R);
-    mark(5);
-    k_alloc<<<gc, 128, 0, s>>>(D, R);
-    mark(6);
-    k_write<<<gc, 128, 0, s>>>(D, R);
-    mark(7);
-    k_relocate<<<g, TB, 0, s>>>(D, R);
-    mark(8);
+    ck(cudaGraphLaunch(gexec, s), "graph launch");
+    launches += uint64_t(rpg) * 12;
+    ck(cudaMemcpyAsync(&hs, W.state.p, sizeof(State), cudaMemcpyDeviceToHost, s), "d2h");
     ck(cudaMemcpyAsync(W.h_ctr, W.ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, s), "d2h");
-    ck(cudaStreamSynchronize(s), "round");
-    Counters h = *W.h_ctr;
-    if (trace >= 3) {
-      float ms[8];
-      for (int i = 0; i < 8; ++i) cudaEventElapsedTime(&ms[i], tev[i], tev[i + 1]);
-      fprintf(stderr, "[wtet-ms] round %u vote %.3f expand %.3f big %.3f resolve %.3f shared %.3f alloc %.3f write %.3f reloc %.3f\n",
-              round, ms[0], ms[1], ms[2], ms[3], ms[4], ms[5], ms[6], ms[7]);
-    }
-    if (trace >= 2 && n_active <= 64) {
-      std::vector<uint32_t> act(n_active);
-      cudaMemcpy(act.data(), W.active.p, n_active * 4, cudaMemcpyDeviceToHost);
-      for (uint32_t a : act) {
-        float4 q;
-        uint32_t l;
-        cudaMemcpy(&q, W.pts.p + a, sizeof(float4), cudaMemcpyDeviceToHost);
-        cudaMemcpy(&l, W.loc.p + a, 4, cudaMemcpyDeviceToHost);
-        fprintf(stderr, "[wtet-pt] round %u p %u loc %u xyz %.6f %.6f %.6f\n", round, a, l, q.x, q.y, q.z);
-      }
-    }
+    ck(cudaStreamSynchronize(s), "rounds");
+    const Counters& h = *W.h_ctr;
     if (trace)
       fprintf(stderr, "[wtet] round %u active %u expanded %llu cand %u inserted %u big %llu alloc %u freed %u top %u err %x\n",
-              round, n_active, (unsigned long long)h.n_expanded, h.n_cand, h.n_inserted,
-              (unsigned long long)h.n_big, h.alloc_used, h.n_freed_next, tet_top, h.err);
-    if (h.err & ~uint32_t(kErrCapacity)) {
+              hs.round, hs.n_active, (unsigned long long)h.n_expanded, h.n_cand, h.n_inserted,
+              (unsigned long long)h.n_big, h.alloc_used, h.n_freed_next, hs.tet_top, h.err);
+    if (hs.stop == 1) {
+      if (gexec) cudaGraphExecDestroy(gexec);
       char buf[160];
-      snprintf(buf, sizeof buf, "device consistency check failed (flags 0x%x) in round %u", h.err, round);
+      snprintf(buf, sizeof buf, "device consistency check failed (flags 0x%x) in round %u", h.err, hs.round);
       throw Error{(h.err & kErrPrec) ? WTET_ERR_PRECISION : WTET_ERR_INTERNAL, buf};
     }
-    st.inserted += h.n_inserted;
-    // Slots: recycled ones not handed out carry over; fresh ones extend the top.
-    uint32_t used = h.alloc_used;
-    uint32_t fresh = used > n_freed_prev ? used - n_freed_prev : 0u;
-    uint32_t left = n_freed_prev > used ? n_freed_prev - used : 0u;
-    if (left)
-      ck(cudaMemcpyAsync(W.freed_b.p + h.n_freed_next, W.freed_a.p + used, size_t(left) * 4,
-                         cudaMemcpyDeviceToDevice, s),
-         "freed carry");
-    tet_top += fresh;
-    n_freed_prev = h.n_freed_next + left;
-    std::swap(W.freed_a, W.freed_b);
-    std::swap(W.active, W.active_next);
-    n_active = h.n_next;
-    if (h.err & kErrCapacity) {
+    if (hs.stop == 3) {
+      if (gexec) cudaGraphExecDestroy(gexec);
+      throw Error{WTET_ERR_NO_CONVERGE, "insertion did not converge within max_insert_iterations"};
+    }
+    if (hs.stop == 2) {
       // Grow the tet arrays (keeping contents); the displaced winners retry.
       uint64_t ncap = std::min<uint64_t>(cap * 3 / 2 + 1024, 0x7FFFFFF0ull);
       if (ncap <= cap) throw Error{WTET_ERR_CAPACITY, "tet capacity exhausted"};
-      W.tv.grow_keep(ncap, tet_top, s, "grow tv");
-      ck(cudaMemsetAsync(W.tv.p + tet_top, 0xFF, (ncap - tet_top) * sizeof(uint4), s), "memset");
-      W.tn.grow_keep(ncap, tet_top, s, "grow tn");
+      const uint32_t top = hs.tet_top;
+      W.tv.grow_keep(ncap, top, s, "grow tv");
+      ck(cudaMemsetAsync(W.tv.p + top, 0xFF, (ncap - top) * sizeof(uint4), s), "memset");
+      W.tn.grow_keep(ncap, top, s, "grow tn");
       W.nslot.grow_keep(ncap, 0, s, "grow nslot");
-      W.ccav.grow_keep(ncap, tet_top, s, "grow ccav");
-      ck(cudaMemsetAsync(W.ccav.p + tet_top, 0xFF, (ncap - tet_top) * 8, s), "memset");
-      W.cring.grow_keep(ncap, tet_top, s, "grow cring");
-      ck(cudaMemsetAsync(W.cring.p + tet_top, 0xFF, (ncap - tet_top) * 8, s), "memset");
-      W.vote.grow_keep(ncap, tet_top, s, "grow vote");
-      ck(cudaMemsetAsync(W.vote.p + tet_top, 0, (ncap - tet_top) * 8, s), "memset");
-      W.freed_a.grow_keep(ncap, n_freed_prev, s, "grow freed");
-      W.freed_b.grow_keep(ncap, 0, s, "grow freed");
+      W.ccav.grow_keep(ncap, top, s, "grow ccav");
+      ck(cudaMemsetAsync(W.ccav.p + top, 0xFF, (ncap - top) * 8, s), "memset");
+      W.cring.grow_keep(ncap, top, s, "grow cring");
+      ck(cudaMemsetAsync(W.cring.p + top, 0xFF, (ncap - top) * 8, s), "memset");
+      W.vote.grow_keep(ncap, top, s, "grow vote");
+      ck(cudaMemsetAsync(W.vote.p + top, 0, (ncap - top) * 8, s), "memset");
+      W.freed_a.grow_keep(ncap, ncap > 0 ? W.freed_a.n : 0, s, "grow freed");
+      W.freed_b.grow_keep(ncap, W.freed_b.n, s, "grow freed");
       W.newid.grow_keep(ncap, 0, s, "grow newid");
       cap = ncap;
+      refresh();
+      hs.stop = 0;
+      ck(cudaMemcpyAsync(W.state.p, &hs, sizeof(State), cudaMemcpyHostToDevice, s), "h2d");
       uint32_t zero = 0;
       ck(cudaMemcpyAsync(&W.ctr.p->err, &zero, 4, cudaMemcpyHostToDevice, s), "clear err");
       ck(cudaStreamSynchronize(s), "grow");
+      build_graph();
+      continue;
     }
-    refresh();
-    D.freed_prev = W.freed_a.p;
-    D.freed_next = W.freed_b.p;
-    D.active = W.active.p;
-    D.active_next = W.active_next.p;
+    if (hs.done) break;
   }
+  if (gexec) cudaGraphExecDestroy(gexec);
+  const uint32_t tet_top = hs.tet_top;
+  const uint32_t round = hs.round;
+  st.strata = hs.strata;
+  st.inserted = hs.inserted;
   st.walk_steps = W.h_ctr->walk_steps;
   st.candidates = W.h_ctr->n_expanded;
   st.big_cavities = W.h_ctr->n_big;
@@ -1459,6 +1799,7 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   ck(cudaMemsetAsync(W.cfill.p, 0, nc * 4, s), "memset");
   uint32_t gt = blocks_for(tet_top, TB, 148 * 32);
   k_count<<<gt, TB, 0, s>>>(D, tet_top, W.ccount.p, W.hullcnt.p, W.hull.p);
+  launches += 1;
   std::vector<uint32_t> ccount(nc);
   ck(cudaMemcpyAsync(ccount.data(), W.ccount.p, nc * 4, cudaMemcpyDeviceToHost, s), "d2h");
   ck(cudaStreamSynchronize(s), "count");
@@ -1476,6 +1817,7 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     k_emit<<<gt, TB, 0, s>>>(D, tet_top, W.newid.p, W.coff.p, d_out_t, d_out_a);
     k_infinity<<<(nc + 127) / 128, 128, 0, s>>>(D, W.ci.p, nc, W.ccount.p, W.hullcnt.p, W.hull.p, W.newid.p,
                                                 W.coff.p, d_out_t, d_out_a);
+    launches += 3;
     ck(cudaGetLastError(), "output kernels");
   }
   ck(cudaEventRecord(W.ev1, s), "event record");
@@ -1489,6 +1831,7 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   float ms = 0.f;
   cudaEventElapsedTime(&ms, W.ev0, W.ev1);
   st.device_ms = ms;
+  st.kernel_launches = launches;
   res.stats = st;
   return res;
 }

@@ -30,10 +30,12 @@ struct Job {
   std::vector<uint64_t> offsets;  // host, num_clouds + 1
   wtet_config cfg{};
   cudaStream_t stream = nullptr;
+  uint32_t rounds_per_graph = 0;  // 0: default
 };
 
 struct JobResult {
   std::vector<uint64_t> tet_offsets;  // host, num_clouds + 1
+  std::vector<uint64_t> failed;       // global input indices of exact duplicates, ascending
   wtet_stats stats{};
 };
 
