@@ -135,6 +135,24 @@ int wtet_delaunay_batched(const float* xyz, const uint64_t* offsets, uint32_t nu
 int wtet_check_quality(const float* xyz, uint64_t n, const uint32_t* tets, const uint32_t* adjacency,
                        uint64_t m, uint64_t* violations, uint64_t* interior_tets);
 
+/* Allocation-free exact quality check.  No counterpart in the reference.
+ * For callers that must not allocate GPU memory during the call -- code that is
+ * recording a CUDA stream capture, serving loops that cannot stall on or
+ * fragment an allocator another framework owns, fixed memory budgets.  Same
+ * result as wtet_check_quality, but d_xyz (n x 3 f32), d_tets and d_adjacency
+ * (m x 4 u32) are device pointers and the scratch (normalised points, box,
+ * counters) is a fixed 16 MiB array in device memory that each GPU holds while
+ * the library is loaded.  n may not exceed WTET_NOALLOC_MAX_POINTS (larger n
+ * returns WTET_ERR_ARG).  The first call on a device looks up that array's
+ * address, so make it before any stream capture.  Calls share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller.
+ * Runs on `stream` (cudaStream_t as void*, NULL = default) and returns when the
+ * counts are ready. */
+#define WTET_NOALLOC_MAX_POINTS 1048576ull
+int wtet_check_quality_noalloc(const float* d_xyz, uint64_t n, const uint32_t* d_tets,
+                               const uint32_t* d_adjacency, uint64_t m, uint64_t* violations,
+                               uint64_t* interior_tets, void* stream);
+
 /* Upper bound on the output tet count for n points (for sizing buffers). */
 uint64_t wtet_max_tets(uint64_t n);
 

@@ -15,7 +15,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libwtet.so")
-SOURCES = ["engine.cu", "capi.cu", "learned.cu", "sort.cu"]
+SOURCES = ["engine.cu", "capi.cu", "noalloc.cu", "learned.cu", "sort.cu"]
 HEADERS = ["exact.cuh", "engine.cuh", "learned.cuh"]
 
 NVCC_FLAGS = [

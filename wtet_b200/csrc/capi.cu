@@ -67,6 +67,11 @@ wtet::JobResult run_dev(const float* d_xyz, const std::vector<uint64_t>& offsets
 
 }  // namespace
 
+namespace wtet {
+// Lets other translation units of the library report through wtet_last_error().
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace wtet
+
 extern "C" {
 
 void wtet_config_default(wtet_config* cfg) {

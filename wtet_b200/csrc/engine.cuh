@@ -53,6 +53,9 @@ uint64_t max_tets_for(uint64_t n);
 
 void release_thread_workspace();
 
+// Message returned by wtet_last_error() on this thread.
+void set_last_error(const std::string& msg);
+
 // Per-thread device buffers reused across calls (grown on demand).
 float* ws_input(size_t nfloats);
 void ws_outputs(size_t rows, uint32_t** tets, uint32_t** adj);

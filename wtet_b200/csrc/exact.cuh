@@ -18,6 +18,8 @@
 
 namespace wtet {
 namespace ex {
+// Internal linkage: every translation unit of the library gets its own copy.
+namespace {
 
 // Error flag bit raised when an expansion would outgrow its fixed buffer.
 constexpr uint32_t kErrPrecision = 1u << 4;
@@ -557,5 +559,6 @@ __device__ __forceinline__ int orient4d_sos(const double* a, const double* b, co
   return orient4d_sos_degenerate(a, b, c, d, e, ia, ib, ic, id, ie, flags);
 }
 
+}  // namespace
 }  // namespace ex
 }  // namespace wtet
