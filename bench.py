@@ -58,6 +58,14 @@ def make_workload(name: str, rank: int = 0, world: int = 1):
 
     if name == "mixture8M":
         return [fx.mixture(8_000_000, 3)]
+    if name == "mixture1M":
+        return [fx.mixture(1_000_000, 3)]
+    if name == "mixture100k":
+        return [fx.mixture(100_000, 3)]
+    if name == "lattice2M":
+        return [fx.lattice(128)]
+    if name == "sphere1M":
+        return [fx.unit_sphere(1_000_000, 2)]
     if name == "uniform8M":
         return [fx.uniform(8_000_000, 1)]
     if name == "batched":
@@ -201,6 +209,14 @@ def run_gpu(args):
                 raise RuntimeError(L.wtet_last_error().decode())
             return int(toff[-1]), st
 
+    if args.profile_once:
+        # one triangulation and nothing else: a short, complete launch list for ncu
+        num, s = step()
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"profile_once": args.workload, "num_tets": num, "rounds": s.rounds,
+                              "kernel_launches": s.kernel_launches, "device_ms": s.device_ms}))
+        return
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -323,6 +339,10 @@ WORKLOADS = {
     "mixture8M": "8,000,000 points: 60% uniform [0,1]^3, 30% Gaussian ball (0.5, sigma 0.1), "
                  "10% thin shell r=0.4 (jitter 1e-4); float32, seed 3",
     "uniform8M": "8,000,000 points uniform in [0,1]^3, float32, seed 1",
+    "mixture1M": "1,000,000 points of the 8M mixture's distribution (profiling size)",
+    "mixture100k": "100,000 points of the 8M mixture's distribution (profiling size)",
+    "lattice2M": "128^3 = 2,097,152 points on the exact lattice float32(i)/127 (SoS stress)",
+    "sphere1M": "1,000,000 points on the unit sphere (normalised Gaussian directions), float32, seed 2",
     "batched": "4,096 clouds, sizes log-uniform in [64, 65536], each uniform / Gaussian / shell / "
                "jittered lattice, float32, seed 4",
 }
@@ -406,6 +426,8 @@ def main():
     ap.add_argument("--vote", default="plain", choices=["plain", "learned"])
     ap.add_argument("--cpu-sample", type=int, default=1_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-once", action="store_true",
+                    help="run a single triangulation and exit (for ncu launch lists)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

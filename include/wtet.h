@@ -61,8 +61,17 @@ typedef struct wtet_config {
   uint32_t max_insert_iterations;  /* cap on insertion rounds per stratum, default 100 */
   uint32_t max_flip_iterations;    /* accepted for compatibility; default 10 */
   uint32_t vote_mode;              /* wtet_vote_mode, default plain */
-  uint32_t block_size;             /* 0 = autotuned / default */
-  uint32_t reserved[7];
+  /* Performance knobs.  0 = autotuned: the installed autotuner table's value
+   * for the job's size bucket (wtet_autotune_set_table), else the default.
+   * None of them changes the triangulation. */
+  uint32_t block_size;             /* threads per block of the per-point kernels: 128, 256 (default), 512 */
+  uint32_t rounds_per_graph;       /* insertion rounds replayed per CUDA-graph launch (default 8, max 64) */
+  uint32_t overlap_shift;          /* next stratum starts when the current one has thinned to
+                                      1/2^overlap_shift of its size (default 3) */
+  uint32_t candidate_filter;       /* neighbourhood pre-claim before cavity growth: 1 = on (default),
+                                      2 = off */
+  uint32_t pool_factor;            /* cavity-pool entries per point (default 24, 4..64) */
+  uint32_t reserved[3];
 } wtet_config;
 
 /* Per-call statistics (the reference prints these as [DEBUG]/[TIMING] lines,
@@ -79,6 +88,7 @@ typedef struct wtet_stats {
   uint64_t num_failed;        /* points left out as exact duplicates */
   uint64_t kernel_launches;   /* CUDA kernels executed by the call (graph nodes included) */
   double device_ms;           /* device time of the call, CUDA events */
+  uint64_t vote_winners;      /* points that won their tet's vote (insertion attempts) */
 } wtet_stats;
 
 /* Host-memory result owned by the library; release with wtet_result_free. */
@@ -152,6 +162,86 @@ int wtet_check_quality(const float* xyz, uint64_t n, const uint32_t* tets, const
 int wtet_check_quality_noalloc(const float* d_xyz, uint64_t n, const uint32_t* d_tets,
                                const uint32_t* d_adjacency, uint64_t m, uint64_t* violations,
                                uint64_t* interior_tets, void* stream);
+
+/* ---- Learned insertion scheduler (no counterpart in the reference, which
+ * orders insertions by the circumsphere determinant alone,
+ * src/shaders/vote.wgsl:401-494).  Every tet votes for its point deepest in
+ * its circumsphere; the winners compete for their cavities, and where two
+ * meet the better claim priority inserts first.  The plain method draws that
+ * priority at random; with vote_mode = WTET_VOTE_LEARNED it is the logit of a
+ * 12 -> 64 -> 64 -> 64 -> 1 ReLU MLP predicting that the winner inserts in its
+ * round.  Only the order of insertions changes: the output is the same tet set.
+ *
+ * Parameters are FP32 in one flat array of WTET_MLP_PARAMS values:
+ * W1[64][12] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] W4[64] b4 (row =
+ * output unit).  Inference rounds weights and activations to BF16 and
+ * accumulates in FP32 on the tensor cores. */
+#define WTET_MLP_FEATURES 12
+#define WTET_MLP_HIDDEN 64
+#define WTET_MLP_PARAMS 9217
+
+/* Installs the weights used by WTET_VOTE_LEARNED (process-wide; uploaded to
+ * each device on its next learned run).  count must be WTET_MLP_PARAMS. */
+int wtet_learned_set_weights(const float* params, uint64_t count);
+/* 1 when weights are installed, else 0. */
+int wtet_learned_has_weights(void);
+
+/* Training data from the plain method's own runs: triangulates the clouds
+ * (layout of wtet_delaunay_batched) with the plain vote and records, for 1 in
+ * 2^sample_shift vote winners, the 12 features (features, capacity x 12) and
+ * whether that winner inserted in that round (labels, capacity).  *count
+ * receives the records written (at most capacity).  The triangulation itself
+ * is computed and discarded. */
+int wtet_learned_collect(const float* xyz, const uint64_t* offsets, uint32_t num_clouds,
+                         const wtet_config* cfg, uint32_t sample_shift, float* features, uint8_t* labels,
+                         uint64_t capacity, uint64_t* count, wtet_stats* stats);
+
+/* Mean binary cross-entropy (logits vs labels in {0,1}) of the FP32 network on
+ * n samples and its gradient with respect to all parameters, computed by the
+ * training kernels (forward + backward on the device, FP32). */
+int wtet_mlp_loss_grad(const float* x, const float* y, uint64_t n, const float* params, float* loss,
+                       float* grads);
+
+typedef struct wtet_train_config {
+  uint32_t epochs;    /* passes over the samples */
+  uint32_t batch;     /* samples per Adam step */
+  float lr;           /* Adam step size */
+  float beta1, beta2; /* Adam moment decays */
+  float eps;          /* Adam epsilon */
+  uint64_t seed;      /* shuffling seed */
+} wtet_train_config;
+
+/* Trains the network on the device (forward and backward kernels, Adam):
+ * params is read as the initial weights and receives the trained ones;
+ * epoch_loss (optional, room for epochs) receives the mean loss per epoch. */
+int wtet_mlp_train(const float* x, const float* y, uint64_t n, const wtet_train_config* tc, float* params,
+                   float* epoch_loss);
+
+/* Scores n feature rows with the installed weights through the same fused
+ * BF16 tensor-core routine the learned vote runs (for testing it). */
+int wtet_mlp_score(const float* x, uint64_t n, float* scores);
+
+/* ---- Autotuner (no reference counterpart).  A table of size buckets, each
+ * with the performance knobs measured fastest for it (wtet_b200.autotune
+ * measures and persists it; the Python package installs its packaged table
+ * on load).  A job uses the first entry of its kind (one cloud, or several)
+ * whose max_points covers its total point count. */
+typedef struct wtet_tune_entry {
+  uint64_t max_points;       /* bucket: jobs with at most this many points in total */
+  uint32_t batched;          /* 0: jobs of one cloud, 1: jobs of several clouds */
+  uint32_t block_size;       /* knob values as in wtet_config (0 = default) */
+  uint32_t rounds_per_graph;
+  uint32_t overlap_shift;
+  uint32_t candidate_filter;
+  uint32_t pool_factor;
+} wtet_tune_entry;
+
+/* Installs the table (process-wide; replaces the previous one; count 0 clears). */
+int wtet_autotune_set_table(const wtet_tune_entry* entries, uint32_t count);
+/* Copies up to capacity entries of the installed table; *count = its size. */
+int wtet_autotune_get_table(wtet_tune_entry* entries, uint32_t capacity, uint32_t* count);
+/* The knobs a job of n points in num_clouds clouds would run with. */
+int wtet_autotune_resolve(const wtet_config* cfg, uint64_t n, uint32_t num_clouds, wtet_config* out);
 
 /* Upper bound on the output tet count for n points (for sizing buffers). */
 uint64_t wtet_max_tets(uint64_t n);

@@ -1,0 +1,183 @@
+"""The learned insertion scheduler: its CPU oracle, the device training
+kernels (gradients against the oracle), the fused BF16 inference (against a
+BF16-emulating restatement), the training log, and the scheduler itself --
+same tet set as the plain method, and the gain it brings."""
+import os
+
+import numpy as np
+import pytest
+
+import fixtures as fx
+from oracle import mlp as OM
+
+
+def _random_params(seed, scale=1.0):
+    r = np.random.default_rng(seed)
+    d = {}
+    for name, shape in OM.SIZES:
+        fan = shape[-1] if len(shape) == 2 else OM.H
+        d[name] = r.normal(0, scale / np.sqrt(fan), shape) if name.startswith("W") else r.normal(0, 0.1, shape)
+    return OM.pack(d)
+
+
+def _samples(n, seed):
+    r = np.random.default_rng(seed)
+    X = r.normal(0, 1, (n, OM.IN)).astype(np.float32)
+    y = (r.random(n) < 0.3).astype(np.float32)
+    return X, y
+
+
+# ---------------------------------------------------------------- CPU ----
+
+def test_oracle_gradient_matches_finite_differences():
+    X, y = _samples(64, 1)
+    p = _random_params(2)
+    loss, g = OM.loss_grad(X, y, p)
+    r = np.random.default_rng(3)
+    for j in r.choice(OM.NUM_PARAMS, 60, replace=False):
+        e = np.zeros(OM.NUM_PARAMS)
+        e[j] = 1e-6
+        num = (OM.loss_grad(X, y, p + e)[0] - OM.loss_grad(X, y, p - e)[0]) / 2e-6
+        assert abs(num - g[j]) <= 1e-6 + 1e-4 * abs(num), (j, num, g[j])
+    assert np.isclose(loss, np.mean(np.logaddexp(0, OM.forward(X, p)) - y * OM.forward(X, p)))
+
+
+def test_bf16_rounding_is_nearest_even():
+    vals = np.array([1.0, 1.0 + 2**-8, 1.0 + 3 * 2**-8, 1.0 + 2**-9, -2.5, 3.0e38], np.float32)
+    want = np.array([1.0, 1.0, 1.0 + 2**-6, 1.0, -2.5, 2.9908e38], np.float32)
+    got = OM.bf16(vals)
+    assert np.array_equal(got[:5], want[:5])
+    assert abs(got[5] / vals[5] - 1) < 2**-8
+
+
+def test_parameter_layout_matches_header(wt):
+    from wtet_b200 import learned
+
+    hdr = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "wtet.h")).read()
+    assert f"#define WTET_MLP_PARAMS {learned.NUM_PARAMS}" in hdr
+    assert f"#define WTET_MLP_FEATURES {learned.NUM_FEATURES}" in hdr
+    assert learned.NUM_PARAMS == OM.NUM_PARAMS
+    assert len(learned.FEATURES) == learned.NUM_FEATURES == OM.IN
+    p = _random_params(4).astype(np.float32)
+    assert np.array_equal(learned.pack(learned.unpack(p)), p)
+
+
+def test_standardisation_folds_into_first_layer(wt):
+    from wtet_b200 import learned
+
+    X, _ = _samples(200, 5)
+    X = X * np.float32(3) + np.float32(1.5)
+    mean, std = X.mean(0).astype(np.float64), X.std(0).astype(np.float64)
+    p = _random_params(6)
+    folded = learned.fold_standardization(p, mean, std)
+    a = OM.forward((X - mean) / std, p)
+    b = OM.forward(X, folded.astype(np.float64))
+    assert np.allclose(a, b, rtol=1e-4, atol=1e-4)
+
+
+def test_packaged_weights_are_valid(wt):
+    from wtet_b200 import learned
+
+    with np.load(learned.DEFAULT_WEIGHTS) as z:
+        p = z["params"]
+        assert p.shape == (learned.NUM_PARAMS,) and p.dtype == np.float32
+        assert np.isfinite(p).all()
+        assert float(z["val_accuracy"]) > float(z["majority"])
+
+
+# ---------------------------------------------------------------- GPU ----
+
+@pytest.mark.gpu
+def test_device_gradients_match_oracle(gpu):
+    from wtet_b200 import learned
+
+    for n, seed in ((1, 7), (37, 8), (3000, 9)):
+        X, y = _samples(n, seed)
+        p = _random_params(seed).astype(np.float32)
+        loss, g = learned.loss_grad(X, y, p)
+        want_loss, want = OM.loss_grad(X, y, p.astype(np.float64))
+        assert abs(loss - want_loss) <= 1e-5 * max(1.0, abs(want_loss))
+        # FP32 kernels against a float64 restatement
+        assert np.abs(g - want).max() <= 1e-5 * np.abs(want).max() + 1e-7, n
+
+
+@pytest.mark.gpu
+def test_fused_inference_matches_bf16_restatement(gpu):
+    from wtet_b200 import learned
+
+    X, _ = _samples(5000, 10)
+    p = _random_params(11).astype(np.float32)
+    learned.set_weights(p)
+    got = learned.score(X)
+    want = OM.score_bf16(X, p)
+    exact = OM.forward(X, p)
+    # BF16 operands with FP32 sums: only the summation order differs from the restatement
+    assert np.abs(got - want).max() <= 2e-3 * max(1.0, np.abs(want).max())
+    # and BF16 stays close to the FP32 network
+    assert np.corrcoef(got, exact)[0, 1] > 0.999
+
+
+@pytest.mark.gpu
+def test_training_is_deterministic_and_learns(gpu):
+    from wtet_b200 import learned
+
+    r = np.random.default_rng(12)
+    X = r.normal(0, 1, (20000, 12)).astype(np.float32)
+    y = ((X[:, 0] - 0.5 * X[:, 3] + 0.25 * X[:, 8] ** 2) > 0.3).astype(np.float32)
+    p1, l1 = learned.train(X, y, epochs=5, batch=1024, lr=3e-3, seed=1)
+    p2, l2 = learned.train(X, y, epochs=5, batch=1024, lr=3e-3, seed=1)
+    assert np.array_equal(p1, p2) and np.array_equal(l1, l2)
+    assert l1[-1] < 0.5 * l1[0]
+    learned.set_weights(p1)
+    acc = ((learned.score(X) > 0) == (y > 0.5)).mean()
+    assert acc > 0.95
+
+
+@pytest.mark.gpu
+def test_collect_records(gpu):
+    from wtet_b200 import learned
+
+    pts = fx.mixture(50_000, 21)
+    X, y, st = learned.collect([pts], sample_shift=0)
+    assert X.shape[0] == y.shape[0] == st["vote_winners"]
+    assert np.isfinite(X).all()
+    assert set(np.unique(y)) <= {0, 1}
+    assert 0.05 < y.mean() < 0.95
+    assert (X[:, 0] >= 0).all() and (X[:, 0] <= 1).all()   # circumcenter distance
+    assert (X[:, 8] >= 0).all() and (X[:, 8] <= 1).all()   # rival neighbours / 4
+    assert set(np.unique(X[:, 11])) <= {0.0, 1.0}          # super-vertex flag
+    # a point inserts once; huge cavities insert outside the recorded winners
+    assert int(y.sum()) <= st["inserted"]
+
+
+LEARNED_CASES = ["cube", "icosahedron", "grid12", "lattice24", "shell5k", "unit_sphere20k", "uniform100k",
+                 "clusters", "mixture50k", "duplicates", "coplanar_offset"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", LEARNED_CASES)
+def test_learned_scheduler_parity(gpu, oracle_mod, name):
+    from test_gpu_parity import CASES, assert_parity
+
+    assert_parity(gpu, oracle_mod, CASES[name](), gpu.Config(vote="learned"))
+
+
+@pytest.mark.gpu
+def test_learned_scheduler_gain(gpu):
+    """What the trained network gains over the plain scheduler on a cloud it
+    was not trained on: fewer insertion rounds and fewer vote winners that
+    fail, for the same tet set."""
+    pts = fx.mixture(1_000_000, 101)
+    plain = gpu.delaunay(pts, gpu.Config())
+    learned = gpu.delaunay(pts, gpu.Config(vote="learned"))
+
+    def canon(t):
+        s = np.sort(t.astype(np.int64), axis=1)
+        return s[np.lexsort(s.T[::-1])]
+
+    assert np.array_equal(canon(plain.tets), canon(learned.tets))
+    sp, sl = plain.stats, learned.stats
+    print(f"plain rounds {sp['rounds']} winners {sp['vote_winners']}; "
+          f"learned rounds {sl['rounds']} winners {sl['vote_winners']}")
+    assert sl["vote_winners"] < 0.9 * sp["vote_winners"]
+    assert sl["rounds"] < sp["rounds"]

@@ -37,7 +37,11 @@ class _Config(ctypes.Structure):
         ("max_flip_iterations", ctypes.c_uint32),
         ("vote_mode", ctypes.c_uint32),
         ("block_size", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 7),
+        ("rounds_per_graph", ctypes.c_uint32),
+        ("overlap_shift", ctypes.c_uint32),
+        ("candidate_filter", ctypes.c_uint32),
+        ("pool_factor", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 3),
     ]
 
 
@@ -54,6 +58,7 @@ class Stats(ctypes.Structure):
         ("num_failed", ctypes.c_uint64),
         ("kernel_launches", ctypes.c_uint64),
         ("device_ms", ctypes.c_double),
+        ("vote_winners", ctypes.c_uint64),
     ]
 
     def as_dict(self):
@@ -85,7 +90,28 @@ EXPORTS = (
     "wtet_initialize_gpu",
     "wtet_gpu_info",
     "wtet_version",
+    "wtet_learned_set_weights",
+    "wtet_learned_has_weights",
+    "wtet_learned_collect",
+    "wtet_mlp_loss_grad",
+    "wtet_mlp_train",
+    "wtet_mlp_score",
+    "wtet_autotune_set_table",
+    "wtet_autotune_get_table",
+    "wtet_autotune_resolve",
 )
+
+
+class TrainConfig(ctypes.Structure):
+    _fields_ = [
+        ("epochs", ctypes.c_uint32),
+        ("batch", ctypes.c_uint32),
+        ("lr", ctypes.c_float),
+        ("beta1", ctypes.c_float),
+        ("beta2", ctypes.c_float),
+        ("eps", ctypes.c_float),
+        ("seed", ctypes.c_uint64),
+    ]
 
 
 def lib_path() -> str:
@@ -130,8 +156,36 @@ def load():
     L.wtet_gpu_info.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
     L.wtet_gpu_info.restype = ctypes.c_int
     L.wtet_version.restype = ctypes.c_char_p
+    L.wtet_learned_set_weights.argtypes = [P, u64]
+    L.wtet_learned_set_weights.restype = ctypes.c_int
+    L.wtet_learned_has_weights.argtypes = []
+    L.wtet_learned_has_weights.restype = ctypes.c_int
+    L.wtet_learned_collect.argtypes = [P, P, ctypes.c_uint32, ctypes.POINTER(_Config), ctypes.c_uint32, P, P, u64,
+                                       ctypes.POINTER(u64), ctypes.POINTER(Stats)]
+    L.wtet_learned_collect.restype = ctypes.c_int
+    L.wtet_mlp_loss_grad.argtypes = [P, P, u64, P, P, P]
+    L.wtet_mlp_loss_grad.restype = ctypes.c_int
+    L.wtet_mlp_train.argtypes = [P, P, u64, ctypes.POINTER(TrainConfig), P, P]
+    L.wtet_mlp_train.restype = ctypes.c_int
+    L.wtet_mlp_score.argtypes = [P, u64, P]
+    L.wtet_mlp_score.restype = ctypes.c_int
+    L.wtet_autotune_set_table.argtypes = [P, ctypes.c_uint32]
+    L.wtet_autotune_set_table.restype = ctypes.c_int
+    L.wtet_autotune_get_table.argtypes = [P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
+    L.wtet_autotune_get_table.restype = ctypes.c_int
+    L.wtet_autotune_resolve.argtypes = [ctypes.POINTER(_Config), u64, ctypes.c_uint32, ctypes.POINTER(_Config)]
+    L.wtet_autotune_resolve.restype = ctypes.c_int
     _lib = L
+    _install_packaged_table()
     return L
+
+
+def _install_packaged_table():
+    """Installs the autotuner table shipped with the package, if present."""
+    if os.path.exists(os.path.join(_HERE, "data", "autotune.json")):
+        from . import autotune
+
+        autotune.load()
 
 
 def _raise(status: int):
@@ -148,13 +202,18 @@ _VOTES = {"plain": 0, "learned": 1}
 class Config:
     """Configuration, as ``wtet.Config`` (src/python.rs:53-117, src/types.rs:32-61).
 
-    ``vote`` ("plain" or "learned") selects the insertion scheduler; every
-    option leaves the resulting triangulation unchanged."""
+    ``vote`` ("plain" or "learned") selects the insertion scheduler;
+    ``block_size``, ``rounds_per_graph``, ``overlap_shift``,
+    ``candidate_filter`` and ``pool_factor`` are performance knobs (0 = the
+    autotuner's value for the job's size, see wtet_b200.autotune).  No option
+    changes the resulting triangulation."""
 
     def __init__(self, insertion_rule: str = "circumcenter", enable_flipping: bool = True,
                  enable_sorting: bool = False, enable_hilbert_sorting: bool = False,
                  enable_splaying: bool = True, max_insert_iterations: int = 100,
-                 max_flip_iterations: int = 10, vote: str = "plain"):
+                 max_flip_iterations: int = 10, vote: str = "plain", block_size: int = 0,
+                 rounds_per_graph: int = 0, overlap_shift: int = 0, candidate_filter: int = 0,
+                 pool_factor: int = 0):
         rule = str(insertion_rule).lower()
         if rule not in _RULES:
             raise ValueError(
@@ -170,8 +229,15 @@ class Config:
         self.max_insert_iterations = int(max_insert_iterations)
         self.max_flip_iterations = int(max_flip_iterations)
         self.vote = vote
+        self.block_size = int(block_size)
+        self.rounds_per_graph = int(rounds_per_graph)
+        self.overlap_shift = int(overlap_shift)
+        self.candidate_filter = int(candidate_filter)
+        self.pool_factor = int(pool_factor)
 
     def _c(self) -> _Config:
+        if self.vote == "learned":
+            _ensure_learned_weights()
         c = _Config()
         c.insertion_rule = _RULES[self.insertion_rule]
         c.enable_flipping = int(self.enable_flipping)
@@ -181,6 +247,11 @@ class Config:
         c.max_insert_iterations = self.max_insert_iterations
         c.max_flip_iterations = self.max_flip_iterations
         c.vote_mode = _VOTES[self.vote]
+        c.block_size = self.block_size
+        c.rounds_per_graph = self.rounds_per_graph
+        c.overlap_shift = self.overlap_shift
+        c.candidate_filter = self.candidate_filter
+        c.pool_factor = self.pool_factor
         return c
 
     def __repr__(self) -> str:
@@ -190,6 +261,14 @@ class Config:
             f"splaying={self.enable_splaying}, max_insert_iter={self.max_insert_iterations}, "
             f"max_flip_iter={self.max_flip_iterations}, vote='{self.vote}')"
         )
+
+
+def _ensure_learned_weights():
+    """Installs the packaged learned-vote weights unless weights are set."""
+    if not load().wtet_learned_has_weights():
+        from . import learned
+
+        learned.load_default()
 
 
 class DelaunayResult:

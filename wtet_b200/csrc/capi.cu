@@ -275,6 +275,32 @@ static int device_string(char* buf, size_t len, bool init) {
   return WTET_OK;
 }
 
+int wtet_autotune_set_table(const wtet_tune_entry* entries, uint32_t count) {
+  if (count && !entries) return fail(WTET_ERR_ARG, "null pointer argument");
+  for (uint32_t i = 0; i < count; ++i) {
+    const wtet_tune_entry& e = entries[i];
+    if (e.batched > 1 || (e.block_size && e.block_size != 128 && e.block_size != 256 && e.block_size != 512) ||
+        e.rounds_per_graph > 64 || e.overlap_shift > 16 || e.candidate_filter > 2 || e.pool_factor > 64)
+      return fail(WTET_ERR_ARG, "autotune entry " + std::to_string(i) + " holds an out-of-range knob");
+  }
+  wtet::set_tune_table(entries, count);
+  return WTET_OK;
+}
+
+int wtet_autotune_get_table(wtet_tune_entry* entries, uint32_t capacity, uint32_t* count) {
+  if (!count || (capacity && !entries)) return fail(WTET_ERR_ARG, "null pointer argument");
+  std::vector<wtet_tune_entry> t = wtet::get_tune_table();
+  *count = uint32_t(t.size());
+  for (uint32_t i = 0; i < capacity && i < t.size(); ++i) entries[i] = t[i];
+  return WTET_OK;
+}
+
+int wtet_autotune_resolve(const wtet_config* cfg, uint64_t n, uint32_t num_clouds, wtet_config* out) {
+  if (!out) return fail(WTET_ERR_ARG, "null pointer argument");
+  *out = wtet::tuned_config(resolve(cfg), n, num_clouds ? num_clouds : 1u);
+  return WTET_OK;
+}
+
 int wtet_initialize_gpu(char* buf, size_t len) { return device_string(buf, len, true); }
 int wtet_gpu_info(char* buf, size_t len) { return device_string(buf, len, false); }
 

@@ -15,9 +15,9 @@
 // Round structure (one insertion round over all clouds of a job):
 //   k_vote        each uninserted point votes for its tet (64-bit atomicMax of
 //                 score | ~point, src/shaders/vote.wgsl semantics)
-//   k_expand      each vote winner grows its cavity by BFS with exact insphere,
-//                 claiming cavity tets and ring tets by 64-bit atomicMin of a
-//                 round-stamped priority key
+//   k_cands/k_bfs each vote winner grows its cavity by warp-cooperative BFS
+//                 with exact insphere, claiming cavity tets by 64-bit atomicMin
+//                 of a round-stamped priority key
 //   k_resolve     a candidate wins when it holds the minimum claim on all its
 //                 cavity tets
 //   k_shared      two winners whose cavities share a face both stay only if
@@ -45,20 +45,20 @@
 
 #include "engine.cuh"
 #include "exact.cuh"
+#include "learned.cuh"
 
 namespace wtet {
 
 constexpr uint32_t NONE = 0xFFFFFFFFu;
 constexpr uint32_t DEAD = 0xFFFFFFFFu;  // tv.x of a retired tet; tv.y then forwards to a live tet
 constexpr uint32_t INS_BIT = 0x80000000u;
-constexpr int SMALL_CAP = 80;           // cavity tets held per thread in the fast path
-// Cavity tiers: a thread with SMALL_CAP tets in registers / local memory, then
-// one warp with BIG_CAP tets in a global slot, then one warp with HUGE_CAP.
+// Cavity tiers: one warp with up to BIG_CAP tets in its scratch region, then
+// one warp with up to HUGE_CAP tets in a global slot.
 constexpr uint32_t BIG_CAP = 1u << 12;
 constexpr uint32_t BIG_SLOTS = 1024;   // large cavities expanded per round
 constexpr uint32_t HUGE_CAP = 1u << 18;
 constexpr uint32_t HUGE_SLOTS = 16;
-// bigflag: tier (0 small, 1 big, 2 huge) | kPending while the tier applies
+// bigflag: tier (0 warp scratch, 2 huge slot) | kPending while the tier applies
 // only from the next round (this round's partial claims carry its key).
 constexpr uint8_t kPending = 0x80;
 constexpr uint8_t kDup = 0x40;  // exact duplicate of an earlier point: never inserted
@@ -108,8 +108,11 @@ struct State {
   uint32_t done;          // all points inserted
   uint32_t stop;          // 1 device error, 2 capacity exhausted, 3 no convergence
   uint32_t max_rounds;
+  uint32_t overlap_shift;
   uint32_t carry_used, carry_left;
+  uint32_t log_used;      // scheduler training records reserved
   unsigned long long inserted;
+  unsigned long long starts;  // vote winners that attempted an insertion
 };
 
 // Everything a kernel needs, passed by value.
@@ -148,7 +151,11 @@ struct Dev {
   uint32_t* cand_base;
   uint8_t* st1;  // candidate owns its whole cavity
   uint8_t* st2;  // ... and no shared face with a better winner is violated
-  uint32_t* bigcand;  // points taking the large-cavity path this round
+  uint32_t* bigcand;  // points taking the huge-cavity path this round
+  uint32_t* starts;   // vote winners expanding their cavity this round
+  unsigned long long* pre;  // neighbourhood pre-claims of the candidates
+  uint32_t prefilter;
+  uint32_t* wscratch; // one BIG_CAP cavity buffer per warp of k_bfs
   uint32_t* pool;
   uint32_t pool_cap;
   uint32_t* big;
@@ -156,10 +163,21 @@ struct Dev {
   uint32_t* freed_next;
   Counters* ctr;
   int rule;
+  // learned scheduler (vote_mode 1) and its training log (vote_mode 2)
+  uint32_t vote_mode;
+  uint32_t* tcount;         // uninserted points per tet this round
+  uint8_t* losses;          // vote wins of each point that did not insert
+  const mlp::Image* mlp;    // inference weights
+  uint16_t* prio;           // claim priority of each vote winner (learned scheduler; null = 0)
+  float* log_x;             // logged features (log_cap x 12)
+  uint8_t* log_y;           // logged labels: the winner inserted this round
+  uint32_t* log_slot;       // log record of each start, NONE if not sampled
+  uint32_t log_cap;
+  uint32_t log_shift;       // keep 1 in 2^log_shift winners
 };
 
 struct RoundArgs {
-  unsigned long long stamp;  // (~round) << 32
+  unsigned long long stamp;  // (~round mod 2^16) << 48
   uint32_t round;
   uint32_t n_active;
   uint32_t n_freed_prev;
@@ -174,7 +192,7 @@ __device__ __forceinline__ RoundArgs load_round(Dev& D) {
   RoundArgs R;
   R.live = !S->done && !S->stop;
   R.round = S->round;
-  R.stamp = (unsigned long long)(~R.round) << 32;
+  R.stamp = (unsigned long long)((~R.round) & 0xFFFFu) << 48;
   R.n_active = R.live ? S->n_active : 0u;
   R.n_freed_prev = S->n_freed_prev;
   R.tet_top = S->tet_top;
@@ -211,9 +229,19 @@ __device__ __forceinline__ uint32_t mix32(uint32_t h) {
   h ^= h >> 16;
   return h;
 }
-__device__ __forceinline__ unsigned long long make_key(const RoundArgs& R, uint32_t p) {
-  return R.stamp | mix32(p ^ (R.round * 0x9E3779B9u));
+// Claim key of candidate p: round stamp (16 bits, decreasing so that a new
+// round's keys beat every stale one), priority (16 bits, 0 = best; the
+// learned scheduler's, else 0) and a bijective hash of p that breaks ties and
+// identifies the owner.  Smaller keys win.
+__device__ __forceinline__ unsigned long long make_key(const Dev& D, const RoundArgs& R, uint32_t p) {
+  const unsigned long long prio = D.prio ? D.prio[p] : 0u;
+  return R.stamp | (prio << 32) | mix32(p ^ (R.round * 0x9E3779B9u));
 }
+
+// Grid-stride loop in which each warp takes one item (warp-uniform).
+#define WARP_LOOP(ci, count)                                                              \
+  for (uint32_t ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ci < (count);         \
+       ci += (gridDim.x * blockDim.x) >> 5)
 
 // Appends `pred` lanes to a list through one atomic per warp.
 __device__ __forceinline__ uint32_t warp_append(uint32_t* ctr, bool pred) {
@@ -586,6 +614,141 @@ __global__ void k_vote(Dev D) {
   }
 }
 
+// Uninserted points per tet for the learned scheduler and its log
+// (warp-aggregated: Morton-ordered neighbours in the list usually share a
+// tet).  Every tet with a count holds a vote winner.  Reset by k_relocate.
+__global__ void k_tcount(Dev D) {
+  const RoundArgs R = load_round(D);
+  if (!R.live) return;
+  for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < R.n_active; i0 += gridDim.x * blockDim.x) {
+    const uint32_t i = i0 + threadIdx.x;
+    uint32_t t = NONE;
+    if (i < R.n_active) {
+      const uint32_t p = D.active[i];
+      if (!(D.bigflag[p] & kDup) && D.loc[p] < D.cap) t = D.loc[p];
+    }
+    const unsigned peers = __match_any_sync(0xFFFFFFFFu, t);
+    if (t != NONE && (threadIdx.x & 31) == uint32_t(__ffs(peers) - 1)) atomicAdd(&D.tcount[t], uint32_t(__popc(peers)));
+  }
+}
+
+// Features of vote winner p in its tet t (vertices V); k_cands has already
+// counted this win in losses[p].
+__device__ __forceinline__ void winner_features(const Dev& D, const RoundArgs& R, uint32_t p, uint32_t t, uint4 V,
+                                                float* f) {
+  const float4 q = D.pts[p];
+  const float depth = vote_score(D.pts, V, q, 0);
+  const CloudInfo C = D.ci[D.vcloud[p]];
+  const uint32_t pn = (p + 1 < C.vbase + C.n) ? p + 1 : p - 1;  // Morton neighbour in the same cloud
+  const float4 r = D.pts[pn];
+  const float dx = r.x - q.x, dy = r.y - q.y, dz = r.z - q.z;
+  const uint4 N = D.tn[t];
+  uint32_t rivals = 0;
+  float crowd = 0.f;
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    const uint32_t nb = comp(N, f);
+    if (nb == NONE || (nb >> 2) >= D.cap) continue;
+    const uint32_t c = D.tcount[nb >> 2];
+    rivals += c ? 1u : 0u;
+    crowd += __log2f(1.f + float(c));
+  }
+  const uint32_t lost = D.losses[p] ? D.losses[p] - 1u : 0u;
+  mlp::features(D.pts[V.x], D.pts[V.y], D.pts[V.z], D.pts[V.w], q, depth, D.tcount[t], lost, R.round,
+                sqrtf(dx * dx + dy * dy + dz * dz), rivals, crowd, f);
+}
+
+// Learned scheduler, after k_cands: the fused tensor-core MLP scores the
+// vote winners (32 per warp, consecutive in the start list), and each winner
+// draws its claim priority as an exponential clock whose rate is the
+// predicted probability w = sigmoid(score) that it inserts: E = -ln(u) / w
+// with u uniform from a hash, smallest E first (weighted random priorities,
+// Efraimidis & Spirakis 2006).  Likely winners go first more often, while the
+// randomness keeps conflict chains short -- a deterministic score order
+// would let insertions advance only as a front through crowded regions.
+// Then the neighbourhood pre-claim of k_cands is made with those keys.
+__global__ void __launch_bounds__(128) k_prio(Dev D) {
+  const RoundArgs R = load_round(D);
+  if (!R.live) return;
+  constexpr int RS = mlp::kRowStride;
+  __shared__ __align__(16) mlp::Smem S;
+  __shared__ __align__(16) uint32_t rows[4][32 * RS];
+  __shared__ float outs[4][32];
+  mlp::load_image(S, D.mlp);
+  __syncthreads();
+  const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t nstart = *(volatile uint32_t*)&D.ctr->big_used;
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + w) * 32; base < nstart; base += warps * 32) {
+    const uint32_t i = base + lane;
+    const bool valid = i < nstart;
+    uint32_t p = 0, t = 0;
+    float f[mlp::kIn];
+#pragma unroll
+    for (int k = 0; k < mlp::kIn; ++k) f[k] = 0.f;
+    if (valid) {
+      p = D.starts[i];
+      t = D.loc[p];
+      winner_features(D, R, p, t, D.tv[t], f);
+    }
+    mlp::stage_row(rows[w] + lane * RS, f);
+    __syncwarp();
+    mlp::score32(S, rows[w], outs[w]);
+    if (valid) {
+      float sc = outs[w][lane];
+      sc = (sc == sc) ? fminf(fmaxf(sc, -20.f), 20.f) : -20.f;
+      const uint32_t h = mix32(p * 0x9E3779B1u ^ (R.round * 0x85EBCA6Bu + 0x165667B1u));
+      const float u = (float(h >> 8) + 0.5f) * (1.f / 16777216.f);
+      const float clock = -__logf(u) * (1.f + __expf(-sc));  // -ln(u) / sigmoid(sc)
+      D.prio[p] = uint16_t(min(f2o(clock) >> 16, 0xFFFFu));
+      if (D.prefilter) {
+        const unsigned long long key = make_key(D, R, p);
+        atomicMin(&D.pre[t], key);
+        const uint4 N = D.tn[t];
+        for (int k = 0; k < 4; ++k) {
+          const uint32_t nb = comp(N, k);
+          if (nb != NONE && (nb >> 2) < D.cap) atomicMin(&D.pre[nb >> 2], key);
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// Scheduler log, after k_cands: features of 1 in 2^log_shift vote winners.
+__global__ void k_log_features(Dev D) {
+  const RoundArgs R = load_round(D);
+  if (!R.live) return;
+  const uint32_t nstart = *(volatile uint32_t*)&D.ctr->big_used;
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nstart; s += gridDim.x * blockDim.x) {
+    const uint32_t p = D.starts[s];
+    uint32_t slot = NONE;
+    const bool keep = (mix32(p ^ (R.round * 0x27D4EB2Fu)) & ((1u << D.log_shift) - 1u)) == 0u;
+    if (keep) {
+      slot = atomicAdd(&D.st->log_used, 1u);
+      if (slot >= D.log_cap) slot = NONE;
+    }
+    D.log_slot[s] = slot;
+    if (slot == NONE) continue;
+    const uint32_t t = D.loc[p];
+    float f[mlp::kIn];
+    winner_features(D, R, p, t, D.tv[t], f);
+#pragma unroll
+    for (int k = 0; k < mlp::kIn; ++k) D.log_x[size_t(slot) * mlp::kIn + k] = f[k];
+  }
+}
+
+// Scheduler log, after k_relocate: label = the winner inserted this round.
+__global__ void k_log_labels(Dev D) {
+  const RoundArgs R = load_round(D);
+  if (!R.live) return;
+  const uint32_t nstart = *(volatile uint32_t*)&D.ctr->big_used;
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nstart; s += gridDim.x * blockDim.x) {
+    const uint32_t slot = D.log_slot[s];
+    if (slot != NONE) D.log_y[slot] = (D.loc[D.starts[s]] & INS_BIT) ? 1 : 0;
+  }
+}
+
 // Inverse of mix32: recovers the point that owns a claim key.
 __device__ __forceinline__ uint32_t unmix32(uint32_t h) {
   h ^= h >> 16;
@@ -599,7 +762,7 @@ __device__ __forceinline__ uint32_t key_owner(const RoundArgs& R, unsigned long 
   return unmix32(uint32_t(key)) ^ (R.round * 0x9E3779B9u);
 }
 __device__ __forceinline__ bool this_round(const RoundArgs& R, unsigned long long key) {
-  return (key >> 32) == (R.stamp >> 32);
+  return (key >> 48) == (R.stamp >> 48);
 }
 
 // Grows the cavity of p (tets whose circumsphere holds p, src/phase2.rs:428-470)
@@ -650,46 +813,156 @@ __device__ int grow_cavity(const Dev& D, uint32_t p, const double* pp, uint32_t 
   return int(K);
 }
 
-__global__ void __launch_bounds__(256) k_expand(Dev D) {
+// Candidates: the vote winner of each tet.  Points whose cavity outgrew the
+// warp scratch in an earlier round go to the huge-cavity path.
+__global__ void k_cands(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
-  uint32_t cav[SMALL_CAP];
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < R.n_active; i += gridDim.x * blockDim.x) {
-    uint32_t p = D.active[i];
-    const uint8_t tier = D.bigflag[p];
-    if (tier & kDup) continue;
-    uint32_t t = D.loc[p];
-    if (t >= D.cap) continue;
-    if (uint32_t(D.vote[t]) != ~p) continue;
-    if (tier) {
-      if (tier == 1) {
-        uint32_t b = atomicAdd(&D.ctr->big_used, 1u);
-        if (b < BIG_SLOTS) D.bigcand[b] = p;
-      } else if (tier == 2) {
-        uint32_t b = atomicAdd(&D.ctr->huge_used, 1u);
-        if (b < HUGE_SLOTS) D.bigcand[BIG_SLOTS + b] = p;
+  for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < R.n_active; i0 += gridDim.x * blockDim.x) {
+    const uint32_t i = i0 + threadIdx.x;
+    bool start = false;
+    uint32_t p = 0;
+    if (i < R.n_active) {
+      p = D.active[i];
+      const uint8_t tier = D.bigflag[p];
+      const uint32_t t = D.loc[p];
+      if (!(tier & kDup) && t < D.cap && uint32_t(D.vote[t]) == ~p) {
+        if (D.losses && D.losses[p] < 255u) D.losses[p] += 1u;
+        if (tier == 2) {
+          uint32_t b = atomicAdd(&D.ctr->huge_used, 1u);
+          if (b < HUGE_SLOTS) D.bigcand[BIG_SLOTS + b] = p;
+        } else if (!tier) {
+          start = true;
+          D.st1[p] = 0;
+          D.st2[p] = 0;
+          if (D.prefilter && !D.prio) {
+            // Pre-claim the tet and its face neighbours: candidates whose
+            // neighbourhoods overlap a better one's would lose their cavity.
+            const unsigned long long key = make_key(D, R, p);
+            atomicMin(&D.pre[t], key);
+            const uint4 N = D.tn[t];
+            for (int f = 0; f < 4; ++f) {
+              const uint32_t nb = comp(N, f);
+              if (nb != NONE && (nb >> 2) < D.cap) atomicMin(&D.pre[nb >> 2], key);
+            }
+          }
+        }
       }
-      continue;
     }
-    D.st1[p] = 0;
-    D.st2[p] = 0;
-    unsigned long long key = make_key(R, p);
+    const uint32_t slot = warp_append(&D.ctr->big_used, start);
+    if (start) D.starts[slot] = p;
+  }
+}
+
+// Warp-cooperative cavity growth: the 32 lanes test the faces of 32 frontier
+// tets at once, so the dependent-load chain of a cavity is its BFS depth, not
+// its size.  The cavity is built in the warp's scratch region, then copied to
+// the pool and registered as a candidate.
+__global__ void __launch_bounds__(128) k_bfs(Dev D) {
+  const RoundArgs R = load_round(D);
+  if (!R.live) return;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  uint32_t* cav = D.wscratch + size_t(warp) * BIG_CAP;
+  const uint32_t nstart = *(volatile uint32_t*)&D.ctr->big_used;
+  WARP_LOOP(si, nstart) {
+    const uint32_t p = D.starts[si];
+    const uint32_t t0 = D.loc[p];
+    const unsigned long long key = make_key(D, R, p);
     double pp[3];
     load_pt(D.pts, p, pp);
-    int K = grow_cavity(D, p, pp, t, key, cav, SMALL_CAP);
-    atomicAdd(&D.ctr->n_expanded, 1ull);
-    if (K < 0) {
-      D.bigflag[p] = kPending | 1;
+    int lost = 0;
+    if (D.prefilter && lane < 5) {
+      uint32_t t = t0;
+      if (lane > 0) {
+        const uint32_t nb = comp(D.tn[t0], lane - 1);
+        t = nb == NONE ? NONE : nb >> 2;
+      }
+      if (t != NONE && t < D.cap && __ldcg(&D.pre[t]) != key) lost = 1;
+    }
+    if (__any_sync(0xFFFFFFFFu, lost)) continue;
+    if (lane == 0) {
+      unsigned long long old = atomicMin(&D.ccav[t0], key);
+      lost = old < key;
+      cav[0] = t0;
+    }
+    lost = __shfl_sync(0xFFFFFFFFu, lost, 0);
+    uint32_t K = 1, head = 0;
+    bool overflow = false;
+    __syncwarp();
+    while (!lost && !overflow && head < K) {
+      const uint32_t idx = head + lane;
+      const bool valid = idx < K;
+      const uint32_t c = valid ? cav[idx] : 0u;
+      const uint4 N = valid ? D.tn[c] : make_uint4(NONE, NONE, NONE, NONE);
+      uint32_t newK = K;
+      bool my_lost = false, my_guard = false;
+      for (int f = 0; f < 4; ++f) {
+        bool add = false;
+        uint32_t nt = 0;
+        const uint32_t nb = comp(N, f);
+        if (valid && nb != NONE) {
+          nt = nb >> 2;
+          if (nt >= D.cap) {
+            my_guard = true;
+          } else if (__ldcg(&D.ccav[nt]) != key && __ldcg(&D.cring[nt]) != key) {
+            const uint4 W = D.tv[nt];
+            if (W.x >= D.nv || W.y >= D.nv || W.z >= D.nv || W.w >= D.nv) {
+              my_guard = true;
+            } else {
+              double P[4][3];
+              load_pt(D.pts, W.x, P[0]);
+              load_pt(D.pts, W.y, P[1]);
+              load_pt(D.pts, W.z, P[2]);
+              load_pt(D.pts, W.w, P[3]);
+              const int sg = o4d_sos(P[0], P[1], P[2], P[3], pp, W.x, W.y, W.z, W.w, p, D.sos, &D.ctr->err);
+              if (sg < 0) {
+                const unsigned long long old = atomicMin(&D.ccav[nt], key);
+                if (old < key) my_lost = true;
+                else if (old != key) add = true;
+              } else {
+                D.cring[nt] = key;  // memo for this candidate only
+              }
+            }
+          }
+        }
+        const unsigned ball = __ballot_sync(0xFFFFFFFFu, add);
+        const uint32_t pos = newK + __popc(ball & ((1u << lane) - 1u));
+        if (add) {
+          if (pos < BIG_CAP) cav[pos] = nt;
+          else overflow = true;
+        }
+        newK += __popc(ball);
+      }
+      if (__any_sync(0xFFFFFFFFu, my_guard)) {
+        if (lane == 0) atomicOr(&D.ctr->err, kErrGuard);
+        lost = 1;
+      }
+      lost |= __any_sync(0xFFFFFFFFu, my_lost);
+      overflow = __any_sync(0xFFFFFFFFu, overflow);
+      head = min(head + 32u, K);
+      K = newK;
+      __syncwarp();
+    }
+    if (lane == 0) atomicAdd(&D.ctr->n_expanded, 1ull);
+    if (overflow) {
+      // Partial claims carry this round's key: the huge path takes it next round.
+      if (lane == 0) D.bigflag[p] = kPending | 2;
       continue;
     }
-    if (K == 0) continue;
-    uint32_t off = atomicAdd(&D.ctr->pool_used, uint32_t(K));
-    if (off + uint32_t(K) > D.pool_cap) continue;  // pool full: retry next round
-    for (int k = 0; k < K; ++k) D.pool[off + k] = cav[k];
-    uint32_t ci = atomicAdd(&D.ctr->n_cand, 1u);
-    D.cand[ci] = p;
-    D.cand_off[ci] = off;
-    D.cand_len[ci] = uint32_t(K);
+    if (lost) continue;
+    uint32_t off = 0;
+    if (lane == 0) off = atomicAdd(&D.ctr->pool_used, K);
+    off = __shfl_sync(0xFFFFFFFFu, off, 0);
+    if (off + K > D.pool_cap) continue;  // pool full: retry next round
+    for (uint32_t k = lane; k < K; k += 32) D.pool[off + k] = cav[k];
+    if (lane == 0) {
+      const uint32_t ci = atomicAdd(&D.ctr->n_cand, 1u);
+      D.cand[ci] = p;
+      D.cand_off[ci] = off;
+      D.cand_len[ci] = K;
+    }
+    __syncwarp();
   }
 }
 
@@ -703,9 +976,6 @@ __device__ __forceinline__ const uint32_t* cand_cavity(const Dev& D, uint32_t of
   return (off & 0x80000000u) ? big_slot(D, off & 0x7FFFFFFFu) : D.pool + off;
 }
 
-#define WARP_LOOP(ci, count)                                                              \
-  for (uint32_t ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ci < (count);         \
-       ci += (gridDim.x * blockDim.x) >> 5)
 
 // Large cavities: one warp per point; the cavity list doubles as the BFS
 // queue and is grown 32 tets at a time.
@@ -713,7 +983,7 @@ __global__ void k_expand_big(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
   const uint32_t lane = threadIdx.x & 31;
-  const uint32_t nbig = min(*(volatile uint32_t*)&D.ctr->big_used, BIG_SLOTS);
+  const uint32_t nbig = 0;  // the warp path of k_bfs covers cavities up to BIG_CAP
   const uint32_t nhuge = min(*(volatile uint32_t*)&D.ctr->huge_used, HUGE_SLOTS);
   WARP_LOOP(wi, nbig + nhuge) {
     const bool huge = wi >= nbig;
@@ -722,7 +992,7 @@ __global__ void k_expand_big(Dev D) {
     uint32_t p = D.bigcand[bi];
     uint32_t t0 = D.loc[p];
     uint32_t* cav = big_slot(D, bi);
-    unsigned long long key = make_key(R, p);
+    unsigned long long key = make_key(D, R, p);
     double pp[3];
     load_pt(D.pts, p, pp);
     int lost = 0;
@@ -819,7 +1089,7 @@ __global__ void k_resolve(Dev D) {
     uint32_t p = D.cand[ci];
     uint32_t K = D.cand_len[ci];
     const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
-    unsigned long long key = make_key(R, p);
+    unsigned long long key = make_key(D, R, p);
     bool ok = true;
     for (uint32_t i = lane; i < K; i += 32)
       if (__ldcg(&D.ccav[cav[i]]) != key) ok = false;
@@ -845,7 +1115,7 @@ __global__ void k_shared(Dev D) {
     }
     uint32_t K = D.cand_len[ci];
     const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
-    unsigned long long key = make_key(R, p);
+    unsigned long long key = make_key(D, R, p);
     bool bad = false;
     double pp[3];
     load_pt(D.pts, p, pp);
@@ -899,7 +1169,7 @@ __global__ void k_alloc(Dev D) {
     if (!D.st2[p]) continue;
     uint32_t K = D.cand_len[ci];
     const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
-    unsigned long long key = make_key(R, p);
+    unsigned long long key = make_key(D, R, p);
     uint32_t Fl = 0;
     for (uint32_t i = lane; i < K; i += 32) {
       uint4 N = D.tn[cav[i]];
@@ -935,21 +1205,79 @@ __global__ void k_alloc(Dev D) {
   }
 }
 
-// Writes the new tets of every winner.  Faces through p are matched by
-// rotating around the boundary edge inside the cavity; a boundary face shared
-// with another winner's cavity links to that winner's new tet.
+// Writes the new tets of every winner.  The three faces through p of a new
+// tet pair up across the boundary edges of the cavity: for cavities of up to
+// kEdgeFaces boundary faces the pairs are matched in a per-warp shared-memory
+// edge table; larger ones rotate around each edge inside the cavity.  A
+// boundary face shared with another winner's cavity links to that winner's
+// new tet.
+constexpr uint32_t kEdgeSlots = 256;  // per warp; load <= 0.47 at kEdgeFaces faces
+constexpr uint32_t kEdgeFaces = 80;
+
+__device__ __forceinline__ uint32_t edge_hash(uint32_t a, uint32_t b) {
+  return mix32(a * 0x9E3779B9u ^ b) & (kEdgeSlots - 1);
+}
+
 __global__ void __launch_bounds__(128) k_write(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
+  __shared__ unsigned long long ekey[4][kEdgeSlots];
+  __shared__ uint32_t ev0[4][kEdgeSlots], ev1[4][kEdgeSlots];
   const uint32_t lane = threadIdx.x & 31;
+  const uint32_t w = threadIdx.x >> 5;
   const uint32_t ncand = *(volatile uint32_t*)&D.ctr->n_cand;
   WARP_LOOP(ci, ncand) {
     uint32_t p = D.cand[ci];
     if (!D.st2[p]) continue;
     uint32_t K = D.cand_len[ci];
     const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
-    unsigned long long key = make_key(R, p);
+    unsigned long long key = make_key(D, R, p);
+    // Boundary faces of the cavity (those with a new slot).
     uint32_t Fl = 0;
+    for (uint32_t i = lane; i < K; i += 32) {
+      const uint4 S = D.nslot[cav[i]];
+      Fl += (S.x != NONE) + (S.y != NONE) + (S.z != NONE) + (S.w != NONE);
+    }
+    uint32_t F = Fl;
+    for (int o = 16; o > 0; o >>= 1) F += __shfl_xor_sync(0xFFFFFFFFu, F, o);
+    const bool use_table = F <= kEdgeFaces;
+    if (use_table) {
+      for (uint32_t j = lane; j < kEdgeSlots; j += 32) {
+        ekey[w][j] = ~0ull;
+        ev0[w][j] = NONE;
+        ev1[w][j] = NONE;
+      }
+      __syncwarp();
+      for (uint32_t i = lane; i < K; i += 32) {
+        const uint32_t c = cav[i];
+        const uint4 V = D.tv[c];
+        const uint4 S = D.nslot[c];
+        for (int f = 0; f < 4; ++f) {
+          const uint32_t sl = comp(S, f);
+          if (sl == NONE) continue;
+          for (int k = 0; k < 4; ++k) {
+            if (k == f) continue;
+            uint32_t e[2];
+            int ne = 0;
+            for (int q = 0; q < 4; ++q)
+              if (q != f && q != k) e[ne++] = comp(V, q);
+            const uint32_t a = min(e[0], e[1]), b = max(e[0], e[1]);
+            const unsigned long long ek = (static_cast<unsigned long long>(a) << 32) | b;
+            const uint32_t val = (sl << 2) | uint32_t(k);
+            uint32_t h = edge_hash(a, b);
+            for (uint32_t probe = 0; probe < kEdgeSlots; ++probe) {
+              const unsigned long long old = atomicCAS(&ekey[w][h], ~0ull, ek);
+              if (old == ~0ull || old == ek) {
+                if (atomicCAS(&ev0[w][h], NONE, val) != NONE) ev1[w][h] = val;
+                break;
+              }
+              h = (h + 1) & (kEdgeSlots - 1);
+            }
+          }
+        }
+      }
+      __syncwarp();
+    }
     bool bad = false;
     for (uint32_t i = lane; i < K; i += 32) {
       uint32_t c = cav[i];
@@ -957,9 +1285,8 @@ __global__ void __launch_bounds__(128) k_write(Dev D) {
       uint4 N = D.tn[c];
       uint4 S = D.nslot[c];
       for (int f = 0; f < 4; ++f) {
-        uint32_t s = comp(S, f);
-        if (s == NONE) continue;
-        ++Fl;
+        uint32_t sl = comp(S, f);
+        if (sl == NONE) continue;
         uint32_t outer = comp(N, f);
         bool shared = false;
         uint32_t link_out = outer;
@@ -980,42 +1307,62 @@ __global__ void __launch_bounds__(128) k_write(Dev D) {
         set_comp(nn, f, link_out);
         for (int k = 0; k < 4; ++k) {
           if (k == f) continue;
-          uint32_t cur = c;
-          uint4 Vc = V;
-          int kc = k, ms = f;
           uint32_t link = NONE;
-          for (int it = 0; it < ROT_LIMIT; ++it) {
-            uint32_t nb = comp(D.tn[cur], kc);
-            if (boundary_face(D, nb, key)) {
-              link = (comp(D.nslot[cur], kc) << 2) | uint32_t(ms);
-              break;
-            }
-            uint32_t nt = nb >> 2;
-            if (nt >= D.cap) break;
-            int entry = int(nb & 3);
-            uint32_t x = comp(Vc, ms);
-            uint4 W = D.tv[nt];
-            int kx = -1;
+          if (use_table) {
+            uint32_t e[2];
+            int ne = 0;
             for (int q = 0; q < 4; ++q)
-              if (comp(W, q) == x) kx = q;
-            if (kx < 0) break;
-            cur = nt;
-            Vc = W;
-            kc = kx;
-            ms = entry;
+              if (q != f && q != k) e[ne++] = comp(V, q);
+            const uint32_t a = min(e[0], e[1]), b = max(e[0], e[1]);
+            const unsigned long long ek = (static_cast<unsigned long long>(a) << 32) | b;
+            const uint32_t mine = (sl << 2) | uint32_t(k);
+            uint32_t h = edge_hash(a, b);
+            for (uint32_t probe = 0; probe < kEdgeSlots; ++probe) {
+              const unsigned long long kk = ekey[w][h];
+              if (kk == ek) {
+                link = ev0[w][h] == mine ? ev1[w][h] : ev0[w][h];
+                break;
+              }
+              if (kk == ~0ull) break;
+              h = (h + 1) & (kEdgeSlots - 1);
+            }
+          } else {
+            uint32_t cur = c;
+            uint4 Vc = V;
+            int kc = k, ms = f;
+            for (int it = 0; it < ROT_LIMIT; ++it) {
+              uint32_t nb = comp(D.tn[cur], kc);
+              if (boundary_face(D, nb, key)) {
+                link = (comp(D.nslot[cur], kc) << 2) | uint32_t(ms);
+                break;
+              }
+              uint32_t nt = nb >> 2;
+              if (nt >= D.cap) break;
+              int entry = int(nb & 3);
+              uint32_t x = comp(Vc, ms);
+              uint4 Wt = D.tv[nt];
+              int kx = -1;
+              for (int q = 0; q < 4; ++q)
+                if (comp(Wt, q) == x) kx = q;
+              if (kx < 0) break;
+              cur = nt;
+              Vc = Wt;
+              kc = kx;
+              ms = entry;
+            }
           }
           if (link == NONE) bad = true;
           set_comp(nn, k, link);
         }
-        D.tv[s] = nv;
-        D.tn[s] = nn;
+        D.tv[sl] = nv;
+        D.tn[sl] = nn;
         // Every vertex on the cavity boundary gets a live incident tet, so a
         // vertex's hint tet is alive whenever it is read (strata activation).
         for (int q = 0; q < 4; ++q)
-          if (q != f) D.vtet[comp(V, q)] = s;
+          if (q != f) D.vtet[comp(V, q)] = sl;
         if (outer != NONE && !shared && (outer >> 2) < D.cap) {
-          uint32_t* w = reinterpret_cast<uint32_t*>(&D.tn[outer >> 2]) + (outer & 3);
-          *w = (s << 2) | uint32_t(f);
+          uint32_t* wp = reinterpret_cast<uint32_t*>(&D.tn[outer >> 2]) + (outer & 3);
+          *wp = (sl << 2) | uint32_t(f);
         }
       }
     }
@@ -1033,15 +1380,15 @@ __global__ void __launch_bounds__(128) k_write(Dev D) {
       D.tv[c] = make_uint4(DEAD, fwd, 0u, 0u);
       D.freed_next[fbase + i] = c;
     }
-    for (int o = 16; o > 0; o >>= 1) Fl += __shfl_xor_sync(0xFFFFFFFFu, Fl, o);
     if (lane == 0) {
       D.vtet[p] = s0;
       D.loc[p] |= INS_BIT;
       D.centry[D.vcloud[p]] = s0;
       D.bigflag[p] = 0;
       atomicAdd(&D.ctr->n_inserted, 1u);
-      atomicAdd(&D.ctr->created, (unsigned long long)Fl);
+      atomicAdd(&D.ctr->created, (unsigned long long)F);
     }
+    __syncwarp();
   }
 }
 
@@ -1067,6 +1414,7 @@ __global__ void k_relocate(Dev D) {
         L |= INS_BIT;
       }
       D.vote[t] = 0ull;
+      if (D.tcount) D.tcount[t] = 0u;
       if (!(L & INS_BIT)) {
         keep = true;
         if (D.bigflag[p] & kPending) D.bigflag[p] &= uint8_t(~kPending);
@@ -1091,7 +1439,8 @@ __global__ void k_begin(Dev D) {
   State* S = D.st;
   if (S->done || S->stop) return;
   S->act_total = 0;
-  while (S->next_level >= 0 && (S->n_active == 0 || 4ull * S->n_active <= S->stratum_size)) {
+  while (S->next_level >= 0 &&
+         (S->n_active == 0 || (uint64_t(S->n_active) << S->overlap_shift) <= S->stratum_size)) {
     const int L = S->next_level--;
     const uint32_t total = D.lvl_total[L];
     if (total == 0) continue;
@@ -1153,6 +1502,7 @@ __global__ void k_end(Dev D) {
   S->par ^= 1u;
   S->n_active = C->n_next;
   S->inserted += C->n_inserted;
+  S->starts += C->big_used + min(C->huge_used, HUGE_SLOTS);
   if (C->err & kErrCapacity) S->stop = 2;
 }
 
@@ -1160,11 +1510,16 @@ __global__ void k_end(Dev D) {
 
 // Counts live tets per cloud and records the hull faces (no neighbour).
 __global__ void k_count(Dev D, uint32_t tet_top, uint32_t* ccount, uint32_t* hullcnt, uint2* hull) {
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < tet_top; t += gridDim.x * blockDim.x) {
-    uint4 V = D.tv[t];
-    if (V.x == DEAD) continue;
-    uint32_t c = D.vcloud[V.x];
-    atomicAdd(&ccount[c], 1u);
+  for (uint32_t t0 = blockIdx.x * blockDim.x; t0 < tet_top; t0 += gridDim.x * blockDim.x) {
+    const uint32_t t = t0 + threadIdx.x;
+    uint4 V = t < tet_top ? D.tv[t] : make_uint4(DEAD, 0, 0, 0);
+    const bool live = V.x != DEAD;
+    const uint32_t c = live ? D.vcloud[V.x] : 0xFFFFFFFFu;
+    // one atomic per (warp, cloud) group
+    const unsigned grp = __match_any_sync(0xFFFFFFFFu, c);
+    const int lane = threadIdx.x & 31;
+    if (live && lane == __ffs(grp) - 1) atomicAdd(&ccount[c], __popc(grp));
+    if (!live) continue;
     uint4 N = D.tn[t];
     for (int f = 0; f < 4; ++f) {
       if (comp(N, f) == NONE) {
@@ -1177,11 +1532,18 @@ __global__ void k_count(Dev D, uint32_t tet_top, uint32_t* ccount, uint32_t* hul
 }
 
 __global__ void k_number(Dev D, uint32_t tet_top, uint32_t* cfill, uint32_t* newid) {
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < tet_top; t += gridDim.x * blockDim.x) {
-    uint4 V = D.tv[t];
-    if (V.x == DEAD) continue;
-    uint32_t c = D.vcloud[V.x];
-    newid[t] = atomicAdd(&cfill[c], 1u);
+  for (uint32_t t0 = blockIdx.x * blockDim.x; t0 < tet_top; t0 += gridDim.x * blockDim.x) {
+    const uint32_t t = t0 + threadIdx.x;
+    uint4 V = t < tet_top ? D.tv[t] : make_uint4(DEAD, 0, 0, 0);
+    const bool live = V.x != DEAD;
+    const uint32_t c = live ? D.vcloud[V.x] : 0xFFFFFFFFu;
+    const unsigned grp = __match_any_sync(0xFFFFFFFFu, c);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(grp) - 1;
+    uint32_t base = 0;
+    if (live && lane == leader) base = atomicAdd(&cfill[c], __popc(grp));
+    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+    if (live) newid[t] = base + __popc(grp & ((1u << lane) - 1u));
   }
 }
 
@@ -1411,10 +1773,10 @@ struct Workspace {
   DBuf<uint32_t> sos, vcloud, vtet, loc;
   DBuf<uint8_t> bigflag;
   DBuf<uint4> tv, tn, nslot;
-  DBuf<unsigned long long> ccav, cring, vote;
+  DBuf<unsigned long long> ccav, cring, vote, pre;
   DBuf<uint32_t> centry, active, active_next, cand, cand_off, cand_len, cand_base, pool, big, freed_a, freed_b;
   DBuf<uint8_t> st1, st2;
-  DBuf<uint32_t> bigcand;
+  DBuf<uint32_t> bigcand, starts, wscratch;
   DBuf<uint64_t> lvl_off;
   DBuf<uint32_t> lvl_total;
   DBuf<State> state;
@@ -1424,6 +1786,9 @@ struct Workspace {
   DBuf<uint64_t> coff;
   DBuf<uint32_t> out_t, out_a, dtab;
   DBuf<uint8_t> dup;
+  DBuf<uint32_t> tcount, log_slot;
+  DBuf<uint8_t> losses;
+  DBuf<uint16_t> prio;
   std::vector<DBuf<uint32_t>> scan_tmp;
   Counters* h_ctr = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -1485,12 +1850,13 @@ void release_thread_workspace() {
   w.xyz.release(); w.off.release(); w.ci.release(); w.mn.release(); w.mx.release();
   w.bucket.release(); w.hist.release(); w.tmp.release(); w.pts.release(); w.sos.release();
   w.vcloud.release(); w.vtet.release(); w.loc.release(); w.bigflag.release(); w.tv.release();
-  w.tn.release(); w.nslot.release(); w.ccav.release(); w.cring.release(); w.vote.release();
+  w.tn.release(); w.nslot.release(); w.ccav.release(); w.cring.release(); w.pre.release(); w.vote.release();
   w.centry.release(); w.active.release(); w.active_next.release(); w.cand.release();
-  w.cand_off.release(); w.cand_len.release(); w.cand_base.release(); w.st1.release(); w.st2.release(); w.bigcand.release(); w.pool.release(); w.big.release();
+  w.cand_off.release(); w.cand_len.release(); w.cand_base.release(); w.st1.release(); w.st2.release(); w.bigcand.release(); w.starts.release(); w.wscratch.release(); w.pool.release(); w.big.release();
   w.freed_a.release(); w.freed_b.release(); w.lvl_off.release(); w.lvl_total.release(); w.state.release(); w.ctr.release();
   w.ccount.release(); w.hullcnt.release(); w.cfill.release(); w.newid.release();
   w.hull.release(); w.coff.release(); w.out_t.release(); w.out_a.release(); w.dtab.release(); w.dup.release();
+  w.tcount.release(); w.log_slot.release(); w.losses.release(); w.prio.release();
   for (auto& b : w.scan_tmp) b.release();
   if (w.h_ctr) cudaFreeHost(w.h_ctr);
   if (w.ev0) cudaEventDestroy(w.ev0);
@@ -1498,6 +1864,135 @@ void release_thread_workspace() {
   if (w.stream) cudaStreamDestroy(w.stream);
   delete tl_ws;
   tl_ws = nullptr;
+}
+
+// ------------------------------------------------- learned-vote weights ----
+
+namespace {
+std::mutex g_mlp_mu;
+std::vector<float> g_mlp_host;  // installed FP32 parameters (empty: none)
+uint64_t g_mlp_version = 0;
+struct MlpDevCopy {
+  int dev;
+  mlp::Image* p;
+  uint64_t version;
+};
+std::vector<MlpDevCopy> g_mlp_dev;
+
+// FP32 -> BF16, round to nearest even (NaN kept quiet).
+uint16_t f2bf(float f) {
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  if ((u & 0x7F800000u) == 0x7F800000u && (u & 0x007FFFFFu)) return uint16_t((u >> 16) | 0x40u);
+  u += 0x7FFFu + ((u >> 16) & 1u);
+  return uint16_t(u >> 16);
+}
+float bf2f(uint16_t h) {
+  uint32_t u = uint32_t(h) << 16;
+  float f;
+  memcpy(&f, &u, 4);
+  return f;
+}
+uint32_t bf_pair(float lo, float hi) { return uint32_t(f2bf(lo)) | (uint32_t(f2bf(hi)) << 16); }
+
+void build_image(const float* P, mlp::Image& I) {
+  using namespace mlp;
+  memset(&I, 0, sizeof I);
+  for (int o = 0; o < kHidden; ++o) {
+    for (int k = 0; k < kIn / 2; ++k)
+      I.w1[o * kW1Stride + k] = bf_pair(P[kOffW1 + o * kIn + 2 * k], P[kOffW1 + o * kIn + 2 * k + 1]);
+    for (int k = 0; k < kHidden / 2; ++k) {
+      I.w2[o * kWStride + k] = bf_pair(P[kOffW2 + o * kHidden + 2 * k], P[kOffW2 + o * kHidden + 2 * k + 1]);
+      I.w3[o * kWStride + k] = bf_pair(P[kOffW3 + o * kHidden + 2 * k], P[kOffW3 + o * kHidden + 2 * k + 1]);
+    }
+    I.w4[o] = bf2f(f2bf(P[kOffW4 + o]));
+    I.b1[o] = P[kOffB1 + o];
+    I.b2[o] = P[kOffB2 + o];
+    I.b3[o] = P[kOffB3 + o];
+  }
+  I.b4 = P[kOffB4];
+}
+}  // namespace
+
+void set_mlp_params(const float* params) {
+  std::lock_guard<std::mutex> g(g_mlp_mu);
+  g_mlp_host.assign(params, params + mlp::kParams);
+  ++g_mlp_version;
+}
+
+bool has_mlp_params() {
+  std::lock_guard<std::mutex> g(g_mlp_mu);
+  return !g_mlp_host.empty();
+}
+
+const void* mlp_image(cudaStream_t s) {
+  std::lock_guard<std::mutex> g(g_mlp_mu);
+  if (g_mlp_host.empty())
+    throw Error{WTET_ERR_ARG, "the learned vote has no weights installed (wtet_learned_set_weights)"};
+  int dev = 0;
+  ck(cudaGetDevice(&dev), "cudaGetDevice");
+  MlpDevCopy* e = nullptr;
+  for (auto& c : g_mlp_dev)
+    if (c.dev == dev) e = &c;
+  if (!e) {
+    mlp::Image* p = nullptr;
+    ck(cudaMalloc(&p, sizeof(mlp::Image)), "learned weights");
+    g_mlp_dev.push_back(MlpDevCopy{dev, p, 0});
+    e = &g_mlp_dev.back();
+  }
+  if (e->version != g_mlp_version) {
+    mlp::Image img;
+    build_image(g_mlp_host.data(), img);
+    ck(cudaMemcpyAsync(e->p, &img, sizeof img, cudaMemcpyHostToDevice, s), "learned weights upload");
+    ck(cudaStreamSynchronize(s), "learned weights upload");
+    e->version = g_mlp_version;
+  }
+  return e->p;
+}
+
+// ------------------------------------------------------------ autotuner ----
+
+namespace {
+std::mutex g_tune_mu;
+std::vector<wtet_tune_entry> g_tune;  // sorted by (batched, max_points)
+}  // namespace
+
+void set_tune_table(const wtet_tune_entry* e, uint32_t count) {
+  std::vector<wtet_tune_entry> t(e, e + count);
+  std::stable_sort(t.begin(), t.end(), [](const wtet_tune_entry& a, const wtet_tune_entry& b) {
+    return a.batched != b.batched ? a.batched < b.batched : a.max_points < b.max_points;
+  });
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  g_tune = std::move(t);
+}
+
+std::vector<wtet_tune_entry> get_tune_table() {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  return g_tune;
+}
+
+// Knobs left at 0 in cfg take the installed table's entry for the job's size
+// bucket (the first entry of its kind whose max_points covers n), then the
+// built-in defaults.  No knob changes the triangulation.
+wtet_config tuned_config(const wtet_config& cfg, uint64_t n, uint32_t nc) {
+  wtet_config c = cfg;
+  const uint32_t batched = nc > 1 ? 1u : 0u;
+  wtet_tune_entry hit{};
+  {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    for (const auto& e : g_tune)
+      if (e.batched == batched && n <= e.max_points) {
+        hit = e;
+        break;
+      }
+  }
+  auto pick = [](uint32_t user, uint32_t table, uint32_t dflt) { return user ? user : (table ? table : dflt); };
+  c.block_size = pick(c.block_size, hit.block_size, 256u);
+  c.rounds_per_graph = pick(c.rounds_per_graph, hit.rounds_per_graph, 8u);
+  c.overlap_shift = pick(c.overlap_shift, hit.overlap_shift, 3u);
+  c.candidate_filter = pick(c.candidate_filter, hit.candidate_filter, 1u);
+  c.pool_factor = pick(c.pool_factor, hit.pool_factor, 24u);
+  return c;
 }
 
 // Kernels with deep exact-arithmetic call chains need a few KB of stack per
@@ -1511,7 +2006,7 @@ void reserve_stack_once() {
   std::lock_guard<std::mutex> g(mu);
   if (dev < 0 || dev >= 64 || done[dev]) return;
   size_t need = 0;
-  const void* ks[] = {(const void*)k_expand, (const void*)k_expand_big, (const void*)k_shared,
+  const void* ks[] = {(const void*)k_bfs, (const void*)k_expand_big, (const void*)k_shared,
                       (const void*)k_relocate, (const void*)k_activate, (const void*)k_init_clouds};
   for (const void* k : ks) {
     cudaFuncAttributes a{};
@@ -1532,8 +2027,12 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   cudaStream_t s = job.stream ? job.stream : W.stream;
   const uint32_t nc = uint32_t(job.offsets.size() - 1);
   const uint64_t n = job.offsets.back();
+  const wtet_config cfg = tuned_config(job.cfg, n, nc);
   if (n + 5ull * nc >= 0x7FFFFFF0ull) throw Error{WTET_ERR_ARG, "too many points for 31-bit vertex ids"};
   JobResult res;
+  // scheduler: 0 plain (random claim priority), 1 learned priority, 2 plain + training log
+  const uint32_t vmode = job.d_log_x ? 2u : (job.cfg.vote_mode == WTET_VOTE_LEARNED ? 1u : 0u);
+  const mlp::Image* mlp_w = vmode == 1 ? static_cast<const mlp::Image*>(mlp_image(s)) : nullptr;
   ck(cudaEventRecord(W.ev0, s), "event record");
 
   // ---- per-cloud layout (host) ----
@@ -1582,8 +2081,11 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   W.cand_base.reserve(n, "cand");
   W.st1.reserve(nv, "status");
   W.bigcand.reserve(BIG_SLOTS + HUGE_SLOTS, "bigcand");
+  W.starts.reserve(n, "starts");
+  W.wscratch.reserve(size_t(148) * 16 * 4 * BIG_CAP, "warp scratch");
   W.st2.reserve(nv, "status");
-  const uint32_t pool_cap = uint32_t(std::min<uint64_t>(std::max<uint64_t>(n * 24, 1 << 16), 1ull << 30));
+  const uint64_t pool_factor = std::min<uint32_t>(std::max<uint32_t>(cfg.pool_factor, 4u), 64u);
+  const uint32_t pool_cap = uint32_t(std::min<uint64_t>(std::max<uint64_t>(n * pool_factor, 1 << 16), 1ull << 30));
   W.pool.reserve(pool_cap, "pool");
   W.big.reserve(size_t(BIG_SLOTS) * BIG_CAP + size_t(HUGE_SLOTS) * HUGE_CAP, "big");
   W.ctr.reserve(1, "counters");
@@ -1601,10 +2103,12 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     W.nslot.reserve(cap, "nslot");
     W.ccav.reserve(cap, "ccav");
     W.cring.reserve(cap, "cring");
+    W.pre.reserve(cap, "pre");
     W.vote.reserve(cap, "vote");
     W.freed_a.reserve(cap, "freed");
     W.freed_b.reserve(cap, "freed");
     W.newid.reserve(cap, "newid");
+    if (vmode) W.tcount.reserve(cap, "tcount");
   };
   reserve_tets(cap0);
   uint64_t cap = cap0;
@@ -1618,7 +2122,18 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   ck(cudaMemsetAsync(W.tv.p, 0xFF, cap * sizeof(uint4), s), "memset");
   ck(cudaMemsetAsync(W.ccav.p, 0xFF, cap * 8, s), "memset");
   ck(cudaMemsetAsync(W.cring.p, 0xFF, cap * 8, s), "memset");
+  ck(cudaMemsetAsync(W.pre.p, 0xFF, cap * 8, s), "memset");
   ck(cudaMemsetAsync(W.vote.p, 0, cap * 8, s), "memset");
+  if (vmode) {
+    W.losses.reserve(nv, "losses");
+    ck(cudaMemsetAsync(W.tcount.p, 0, cap * 4, s), "memset");
+    ck(cudaMemsetAsync(W.losses.p, 0, nv, s), "memset");
+  }
+  if (vmode == 2) W.log_slot.reserve(n, "log slots");
+  if (vmode == 1) {
+    W.prio.reserve(nv, "priorities");
+    ck(cudaMemsetAsync(W.prio.p, 0, nv * 2, s), "memset");
+  }
 
   Dev D{};
   auto refresh = [&]() {
@@ -1626,12 +2141,24 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     D.bigflag = W.bigflag.p; D.tv = W.tv.p; D.tn = W.tn.p; D.ccav = W.ccav.p; D.cring = W.cring.p;
     D.nslot = W.nslot.p; D.vote = W.vote.p; D.cap = uint32_t(cap); D.nv = uint32_t(nv); D.centry = W.centry.p;
     D.active = W.active.p; D.active_next = W.active_next.p; D.cand = W.cand.p; D.cand_off = W.cand_off.p;
-    D.cand_len = W.cand_len.p; D.cand_base = W.cand_base.p; D.st1 = W.st1.p; D.st2 = W.st2.p; D.bigcand = W.bigcand.p; D.pool = W.pool.p; D.pool_cap = pool_cap; D.big = W.big.p;
+    D.cand_len = W.cand_len.p; D.cand_base = W.cand_base.p; D.st1 = W.st1.p; D.st2 = W.st2.p; D.bigcand = W.bigcand.p;
+    D.starts = W.starts.p; D.wscratch = W.wscratch.p; D.pre = W.pre.p;
+    D.prefilter = cfg.candidate_filter == 2 ? 0u : 1u; D.pool = W.pool.p; D.pool_cap = pool_cap; D.big = W.big.p;
     D.freed_prev = W.freed_a.p; D.freed_next = W.freed_b.p; D.ctr = W.ctr.p;
     D.st = W.state.p; D.act[0] = W.active.p; D.act[1] = W.active_next.p;
     D.freed[0] = W.freed_a.p; D.freed[1] = W.freed_b.p; D.ci = W.ci.p; D.lvl_off = W.lvl_off.p;
     D.lvl_total = W.lvl_total.p; D.nc = nc;
     D.rule = int(job.cfg.insertion_rule == WTET_RULE_CENTROID ? 1 : 0);
+    D.vote_mode = vmode;
+    D.tcount = vmode ? W.tcount.p : nullptr;
+    D.losses = vmode ? W.losses.p : nullptr;
+    D.mlp = mlp_w;
+    D.prio = vmode == 1 ? W.prio.p : nullptr;
+    D.log_x = job.d_log_x;
+    D.log_y = job.d_log_y;
+    D.log_slot = vmode == 2 ? W.log_slot.p : nullptr;
+    D.log_cap = uint32_t(std::min<uint64_t>(job.log_cap, 0xFFFFFFF0ull));
+    D.log_shift = std::min<uint32_t>(job.log_shift, 31u);
   };
   refresh();
 
@@ -1679,13 +2206,15 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
 
   wtet_stats st{};
   // max_insert_iterations bounds the rounds of each stratum (src/types.rs:44-46).
-  const uint32_t max_rounds = std::max<uint32_t>(job.cfg.max_insert_iterations, 1u) * (maxtop + 1);
+  // (the claim key holds a 16-bit round stamp)
+  const uint32_t max_rounds = uint32_t(std::min<uint64_t>(
+      uint64_t(std::max<uint32_t>(job.cfg.max_insert_iterations, 1u)) * (maxtop + 1), 65000ull));
   const char* tr = getenv("WTET_TRACE");
   const int trace = tr ? atoi(tr) : 0;
   cudaEvent_t tev[12];
   if (trace >= 3)
     for (auto& e : tev) cudaEventCreate(&e);
-  const uint32_t TB = 256;
+  const uint32_t TB = (cfg.block_size == 128 || cfg.block_size == 512) ? cfg.block_size : 256u;
 
   // ---- the round loop, driven from device state and replayed from a graph ----
   std::vector<uint32_t> lt(maxtop + 1);
@@ -1695,6 +2224,7 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   S0.tet_top = nc;
   S0.next_level = int32_t(maxtop);
   S0.max_rounds = max_rounds;
+  S0.overlap_shift = std::min<uint32_t>(cfg.overlap_shift, 16u);
   ck(cudaMemcpyAsync(W.state.p, &S0, sizeof(State), cudaMemcpyHostToDevice, s), "h2d");
   ck(cudaMemsetAsync(W.ctr.p, 0, sizeof(Counters), s), "memset");
 
@@ -1704,19 +2234,24 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   auto enqueue_round = [&]() {
     k_begin<<<1, 32, 0, s>>>(D);
     k_activate<<<GT, TB, 0, s>>>(D);
+    if (vmode) k_tcount<<<GT, TB, 0, s>>>(D);
     k_vote<<<GT, TB, 0, s>>>(D);
-    k_expand<<<GT, TB, 0, s>>>(D);
+    k_cands<<<GT, TB, 0, s>>>(D);
+    if (vmode == 1) k_prio<<<148 * 4, 128, 0, s>>>(D);
+    if (vmode == 2) k_log_features<<<GT, TB, 0, s>>>(D);
+    k_bfs<<<GW, 128, 0, s>>>(D);
     k_expand_big<<<GB, 128, 0, s>>>(D);
     k_resolve<<<GW, 128, 0, s>>>(D);
     k_shared<<<GW, 128, 0, s>>>(D);
     k_alloc<<<GW, 128, 0, s>>>(D);
     k_write<<<GW, 128, 0, s>>>(D);
     k_relocate<<<GT, TB, 0, s>>>(D);
+    if (vmode == 2) k_log_labels<<<GT, TB, 0, s>>>(D);
     k_carry<<<148, TB, 0, s>>>(D);
     k_end<<<1, 32, 0, s>>>(D);
   };
   // Rounds per host check (the graph holds this many rounds).
-  uint32_t rpg = job.rounds_per_graph ? job.rounds_per_graph : 8u;
+  uint32_t rpg = std::min<uint32_t>(cfg.rounds_per_graph, 64u);
   if (trace) rpg = 1;
   cudaGraphExec_t gexec = nullptr;
   auto build_graph = [&]() {
@@ -1733,7 +2268,7 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   State hs{};
   for (;;) {
     ck(cudaGraphLaunch(gexec, s), "graph launch");
-    launches += uint64_t(rpg) * 12;
+    launches += uint64_t(rpg) * (13 + (vmode == 1 ? 2 : vmode == 2 ? 3 : 0));
     ck(cudaMemcpyAsync(&hs, W.state.p, sizeof(State), cudaMemcpyDeviceToHost, s), "d2h");
     ck(cudaMemcpyAsync(W.h_ctr, W.ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, s), "d2h");
     ck(cudaStreamSynchronize(s), "rounds");
@@ -1765,11 +2300,17 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
       ck(cudaMemsetAsync(W.ccav.p + top, 0xFF, (ncap - top) * 8, s), "memset");
       W.cring.grow_keep(ncap, top, s, "grow cring");
       ck(cudaMemsetAsync(W.cring.p + top, 0xFF, (ncap - top) * 8, s), "memset");
+      W.pre.grow_keep(ncap, top, s, "grow pre");
+      ck(cudaMemsetAsync(W.pre.p + top, 0xFF, (ncap - top) * 8, s), "memset");
       W.vote.grow_keep(ncap, top, s, "grow vote");
       ck(cudaMemsetAsync(W.vote.p + top, 0, (ncap - top) * 8, s), "memset");
       W.freed_a.grow_keep(ncap, ncap > 0 ? W.freed_a.n : 0, s, "grow freed");
       W.freed_b.grow_keep(ncap, W.freed_b.n, s, "grow freed");
       W.newid.grow_keep(ncap, 0, s, "grow newid");
+      if (vmode) {
+        W.tcount.grow_keep(ncap, 0, s, "grow tcount");
+        ck(cudaMemsetAsync(W.tcount.p, 0, ncap * 4, s), "memset");
+      }
       cap = ncap;
       refresh();
       hs.stop = 0;
@@ -1792,6 +2333,8 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   st.big_cavities = W.h_ctr->n_big;
   st.tets_created = W.h_ctr->created;
   st.rounds = round;
+  st.vote_winners = hs.starts;
+  res.logged = std::min<uint64_t>(hs.log_used, job.log_cap);
 
   // ---- output: per-cloud numbering, rows, infinity tets ----
   ck(cudaMemsetAsync(W.ccount.p, 0, nc * 4, s), "memset");

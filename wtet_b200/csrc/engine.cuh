@@ -30,13 +30,20 @@ struct Job {
   std::vector<uint64_t> offsets;  // host, num_clouds + 1
   wtet_config cfg{};
   cudaStream_t stream = nullptr;
-  uint32_t rounds_per_graph = 0;  // 0: default
+  // Training log of the learned scheduler (recorded when d_log_x is set):
+  // features (log_cap x 12 f32) and labels (log_cap u8) of 1 in 2^log_shift
+  // vote winners.
+  float* d_log_x = nullptr;
+  uint8_t* d_log_y = nullptr;
+  uint64_t log_cap = 0;
+  uint32_t log_shift = 0;
 };
 
 struct JobResult {
   std::vector<uint64_t> tet_offsets;  // host, num_clouds + 1
   std::vector<uint64_t> failed;       // global input indices of exact duplicates, ascending
   wtet_stats stats{};
+  uint64_t logged = 0;  // training records written (<= log_cap)
 };
 
 // Triangulates on the device; output written to d_tets / d_adj (device, row
@@ -52,6 +59,19 @@ void check_quality_device(const float* d_xyz, uint64_t n, const uint32_t* d_tets
 uint64_t max_tets_for(uint64_t n);
 
 void release_thread_workspace();
+
+// Learned-vote weights: FP32 parameters in the flat layout of learned.cuh,
+// converted to the BF16 device image and uploaded to each device on first use.
+void set_mlp_params(const float* params);
+bool has_mlp_params();
+// Device image of the installed weights on the current device (uploads on
+// `stream` when stale); throws when no weights are installed.
+const void* mlp_image(cudaStream_t stream);
+
+// Autotuner table (wtet_autotune_set_table) and the knob resolution it drives.
+void set_tune_table(const wtet_tune_entry* entries, uint32_t count);
+std::vector<wtet_tune_entry> get_tune_table();
+wtet_config tuned_config(const wtet_config& cfg, uint64_t n, uint32_t num_clouds);
 
 // Message returned by wtet_last_error() on this thread.
 void set_last_error(const std::string& msg);
