@@ -890,18 +890,18 @@ __global__ void __launch_bounds__(128) k_bfs(Dev D) {
     uint32_t K = 1, head = 0;
     bool overflow = false;
     __syncwarp();
+    // Each pass tests 32 (frontier tet, face) pairs, one per lane: 8 queued
+    // tets x 4 faces, so a small frontier costs one dependent load chain per
+    // pass instead of one per face.
     while (!lost && !overflow && head < K) {
-      const uint32_t idx = head + lane;
-      const bool valid = idx < K;
-      const uint32_t c = valid ? cav[idx] : 0u;
-      const uint4 N = valid ? D.tn[c] : make_uint4(NONE, NONE, NONE, NONE);
-      uint32_t newK = K;
-      bool my_lost = false, my_guard = false;
-      for (int f = 0; f < 4; ++f) {
-        bool add = false;
-        uint32_t nt = 0;
-        const uint32_t nb = comp(N, f);
-        if (valid && nb != NONE) {
+      const uint32_t idx = head + (lane >> 2);
+      const uint32_t f = lane & 3u;
+      bool add = false, my_lost = false, my_guard = false;
+      uint32_t nt = 0;
+      if (idx < K) {
+        const uint32_t c = cav[idx];
+        const uint32_t nb = reinterpret_cast<const uint32_t*>(D.tn + c)[f];
+        if (nb != NONE) {
           nt = nb >> 2;
           if (nt >= D.cap) {
             my_guard = true;
@@ -926,13 +926,12 @@ __global__ void __launch_bounds__(128) k_bfs(Dev D) {
             }
           }
         }
-        const unsigned ball = __ballot_sync(0xFFFFFFFFu, add);
-        const uint32_t pos = newK + __popc(ball & ((1u << lane) - 1u));
-        if (add) {
-          if (pos < BIG_CAP) cav[pos] = nt;
-          else overflow = true;
-        }
-        newK += __popc(ball);
+      }
+      const unsigned ball = __ballot_sync(0xFFFFFFFFu, add);
+      const uint32_t pos = K + __popc(ball & ((1u << lane) - 1u));
+      if (add) {
+        if (pos < BIG_CAP) cav[pos] = nt;
+        else overflow = true;
       }
       if (__any_sync(0xFFFFFFFFu, my_guard)) {
         if (lane == 0) atomicOr(&D.ctr->err, kErrGuard);
@@ -940,8 +939,8 @@ __global__ void __launch_bounds__(128) k_bfs(Dev D) {
       }
       lost |= __any_sync(0xFFFFFFFFu, my_lost);
       overflow = __any_sync(0xFFFFFFFFu, overflow);
-      head = min(head + 32u, K);
-      K = newK;
+      head = min(head + 8u, K);
+      K += __popc(ball);
       __syncwarp();
     }
     if (lane == 0) atomicAdd(&D.ctr->n_expanded, 1ull);
@@ -1119,24 +1118,25 @@ __global__ void k_shared(Dev D) {
     bool bad = false;
     double pp[3];
     load_pt(D.pts, p, pp);
-    for (uint32_t i = lane; i < K && !bad; i += 32) {
-      uint32_t c = cav[i];
-      uint4 N = D.tn[c];
-      for (int f = 0; f < 4; ++f) {
-        uint32_t nb = comp(N, f);
+    // one lane per (cavity tet, face)
+    for (uint32_t e = lane; e < 4 * K && !bad; e += 32) {
+      const uint32_t c = cav[e >> 2];
+      const int f = int(e & 3u);
+      {
+        uint32_t nb = reinterpret_cast<const uint32_t*>(D.tn + c)[f];
         if (nb == NONE) continue;
         unsigned long long cc = __ldcg(&D.ccav[nb >> 2]);
         if (cc >= key || !this_round(R, cc)) continue;
         uint32_t q = key_owner(R, cc);
         if (q >= D.nv || !D.st1[q]) continue;
-        uint4 V = D.tv[c];
-        uint32_t w[4] = {V.x, V.y, V.z, V.w};
+        const uint4 V = D.tv[c];
+        uint32_t w[4];
         double P[4][3];
-        for (int k = 0; k < 4; ++k) load_pt(D.pts, w[k], P[k]);
-        P[f][0] = pp[0];
-        P[f][1] = pp[1];
-        P[f][2] = pp[2];
-        w[f] = p;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {  // the new tet on face f: p replaces vertex f
+          w[k] = k == f ? p : comp(V, k);
+          load_pt(D.pts, w[k], P[k]);
+        }
         double qq[3];
         load_pt(D.pts, q, qq);
         if (o4d_sos(P[0], P[1], P[2], P[3], qq, w[0], w[1], w[2], w[3], q, D.sos, &D.ctr->err) < 0) {
@@ -1248,13 +1248,13 @@ __global__ void __launch_bounds__(128) k_write(Dev D) {
         ev1[w][j] = NONE;
       }
       __syncwarp();
-      for (uint32_t i = lane; i < K; i += 32) {
-        const uint32_t c = cav[i];
+      for (uint32_t e = lane; e < 4 * K; e += 32) {
+        const uint32_t c = cav[e >> 2];
+        const int f = int(e & 3u);
+        const uint32_t sl = reinterpret_cast<const uint32_t*>(D.nslot + c)[f];
+        if (sl == NONE) continue;
         const uint4 V = D.tv[c];
-        const uint4 S = D.nslot[c];
-        for (int f = 0; f < 4; ++f) {
-          const uint32_t sl = comp(S, f);
-          if (sl == NONE) continue;
+        {
           for (int k = 0; k < 4; ++k) {
             if (k == f) continue;
             uint32_t e[2];
@@ -1279,15 +1279,15 @@ __global__ void __launch_bounds__(128) k_write(Dev D) {
       __syncwarp();
     }
     bool bad = false;
-    for (uint32_t i = lane; i < K; i += 32) {
-      uint32_t c = cav[i];
-      uint4 V = D.tv[c];
-      uint4 N = D.tn[c];
-      uint4 S = D.nslot[c];
-      for (int f = 0; f < 4; ++f) {
-        uint32_t sl = comp(S, f);
-        if (sl == NONE) continue;
-        uint32_t outer = comp(N, f);
+    // one lane per (cavity tet, face): a boundary face becomes one new tet
+    for (uint32_t e = lane; e < 4 * K; e += 32) {
+      const uint32_t c = cav[e >> 2];
+      const int f = int(e & 3u);
+      const uint32_t sl = reinterpret_cast<const uint32_t*>(D.nslot + c)[f];
+      if (sl == NONE) continue;
+      const uint4 V = D.tv[c];
+      {
+        uint32_t outer = reinterpret_cast<const uint32_t*>(D.tn + c)[f];
         bool shared = false;
         uint32_t link_out = outer;
         if (outer != NONE) {
