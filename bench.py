@@ -38,7 +38,6 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
-sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 METRIC = "Mpoints/s on 1 B200 (exact 3D Delaunay, bit-identical tet set)"
 UNIT = "Mpoints/s"
@@ -54,22 +53,26 @@ def peaks():
 
 
 def make_workload(name: str, rank: int = 0, world: int = 1):
-    import fixtures as fx
+    from wtet_b200 import synthetic as syn
 
     if name == "mixture8M":
-        return [fx.mixture(8_000_000, 3)]
+        return [syn.mixture(8_000_000, 3)]
+    if name == "mixture8M_new":
+        return [syn.mixture(8_000_000, 101)]
     if name == "mixture1M":
-        return [fx.mixture(1_000_000, 3)]
+        return [syn.mixture(1_000_000, 3)]
     if name == "mixture100k":
-        return [fx.mixture(100_000, 3)]
+        return [syn.mixture(100_000, 3)]
     if name == "lattice2M":
-        return [fx.lattice(128)]
+        return [syn.lattice(128)]
     if name == "sphere1M":
-        return [fx.unit_sphere(1_000_000, 2)]
+        return [syn.unit_sphere(1_000_000, 2)]
     if name == "uniform8M":
-        return [fx.uniform(8_000_000, 1)]
+        return [syn.uniform(8_000_000, 1)]
+    if name == "uniform100k":
+        return [syn.uniform(100_000, 1)]
     if name == "batched":
-        clouds = fx.batched_clouds(4096, 4)
+        clouds = syn.batched_clouds(4096, 4)
         return clouds[rank::world]
     raise SystemExit(f"unknown workload {name}")
 
@@ -323,6 +326,8 @@ def run_gpu(args):
     }
     if rank == 0 and not args.no_cpu_baseline and len(clouds) == 1:
         result["cpu_baseline"] = cpu_baseline(clouds[0], args.cpu_sample)
+    if world == 1 and args.variants and args.workload == "mixture8M" and args.vote == "plain":
+        result["variants"] = variants(wt, args)
     if rank == 0:
         print(json.dumps(result), flush=True)
     if world > 1:
@@ -339,13 +344,67 @@ WORKLOADS = {
     "mixture8M": "8,000,000 points: 60% uniform [0,1]^3, 30% Gaussian ball (0.5, sigma 0.1), "
                  "10% thin shell r=0.4 (jitter 1e-4); float32, seed 3",
     "uniform8M": "8,000,000 points uniform in [0,1]^3, float32, seed 1",
+    "mixture8M_new": "the 8M mixture's distribution from a seed no training run saw (seed 101)",
     "mixture1M": "1,000,000 points of the 8M mixture's distribution (profiling size)",
+    "uniform100k": "100,000 points uniform in [0,1]^3, float32, seed 1 (the small plain configuration)",
     "mixture100k": "100,000 points of the 8M mixture's distribution (profiling size)",
     "lattice2M": "128^3 = 2,097,152 points on the exact lattice float32(i)/127 (SoS stress)",
     "sphere1M": "1,000,000 points on the unit sphere (normalised Gaussian directions), float32, seed 2",
     "batched": "4,096 clouds, sizes log-uniform in [64, 65536], each uniform / Gaussian / shell / "
                "jittered lattice, float32, seed 4",
 }
+
+
+def _canon_digest(tets):
+    import hashlib
+
+    t = np.sort(np.asarray(tets, np.int64), axis=1)
+    return hashlib.sha256(t[np.lexsort(t.T[::-1])].tobytes()).hexdigest()
+
+
+def variants(wt, args):
+    """The metric's other two forms, each on its own configuration, device
+    time (CUDA events inside the library), with the tet sets compared:
+    learned vs plain scheduler on 8M mixture points from an unseen seed, and
+    4,096 batched clouds in one call vs looping the plain path over them."""
+    out = {}
+    reps = max(2, min(args.steps, 3))
+    pts = make_workload("mixture8M_new")[0]
+    res = {}
+    for vote in ("plain", "learned"):
+        cfg = wt.Config(vote=vote)
+        wt.delaunay(pts, cfg)
+        runs = [wt.delaunay(pts, cfg) for _ in range(reps)]
+        ms = float(np.median([r.stats["device_ms"] for r in runs]))
+        res[vote] = (runs[-1], ms)
+    same = _canon_digest(res["plain"][0].tets) == _canon_digest(res["learned"][0].tets)
+    out["learned"] = {
+        "workload": "mixture8M_new", "same_tet_set": same,
+        **{f"{v}_{k}": val for v in ("plain", "learned") for k, val in (
+            ("mpts", round(len(pts) / (res[v][1] * 1e3), 3)),
+            ("device_ms", round(res[v][1], 2)),
+            ("rounds", int(res[v][0].stats["rounds"])),
+            ("vote_winners", int(res[v][0].stats["vote_winners"])),
+            ("cavity_searches", int(res[v][0].stats["candidates"])))},
+    }
+    clouds = make_workload("batched")
+    n = sum(len(c) for c in clouds)
+    wt.delaunay_batched(clouds)
+    bms = []
+    for _ in range(reps):
+        rb = wt.delaunay_batched(clouds)
+        bms.append(rb[0].stats["device_ms"])
+    loop_ms = 0.0
+    same_b = True
+    for c, r in zip(clouds, rb):
+        ra = wt.delaunay(c)
+        loop_ms += ra.stats["device_ms"]
+        same_b = same_b and _canon_digest(ra.tets) == _canon_digest(r.tets)
+    bm = float(np.median(bms))
+    out["batched"] = {"workload": "batched", "clouds": len(clouds), "points": n, "same_tet_sets": same_b,
+                      "batched_mpts": round(n / (bm * 1e3), 3), "batched_device_ms": round(bm, 1),
+                      "looped_plain_mpts": round(n / (loop_ms * 1e3), 3), "looped_device_ms": round(loop_ms, 1)}
+    return out
 
 
 def cpu_baseline(points, sample: int):
@@ -424,7 +483,9 @@ def main():
     ap.add_argument("--impl", default="wtet_b200", choices=["wtet_b200", "reference"])
     ap.add_argument("--workload", default="mixture8M", choices=sorted(WORKLOADS))
     ap.add_argument("--vote", default="plain", choices=["plain", "learned"])
-    ap.add_argument("--cpu-sample", type=int, default=1_000_000)
+    ap.add_argument("--cpu-sample", type=int, default=2_000_000)
+    ap.add_argument("--no-variants", dest="variants", action="store_false",
+                    help="skip the learned-scheduler and batched measurements")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-once", action="store_true",
                     help="run a single triangulation and exit (for ncu launch lists)")

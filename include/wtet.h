@@ -71,7 +71,10 @@ typedef struct wtet_config {
   uint32_t candidate_filter;       /* neighbourhood pre-claim before cavity growth: 1 = on (default),
                                       2 = off */
   uint32_t pool_factor;            /* cavity-pool entries per point (default 24, 4..64) */
-  uint32_t reserved[3];
+  uint32_t participation;          /* learned scheduler: a vote winner competes with probability
+                                      min(1, participation/16 * predicted insert probability);
+                                      0 = default (40, i.e. 2.5) */
+  uint32_t reserved[2];
 } wtet_config;
 
 /* Per-call statistics (the reference prints these as [DEBUG]/[TIMING] lines,
@@ -167,10 +170,11 @@ int wtet_check_quality_noalloc(const float* d_xyz, uint64_t n, const uint32_t* d
  * orders insertions by the circumsphere determinant alone,
  * src/shaders/vote.wgsl:401-494).  Every tet votes for its point deepest in
  * its circumsphere; the winners compete for their cavities, and where two
- * meet the better claim priority inserts first.  The plain method draws that
- * priority at random; with vote_mode = WTET_VOTE_LEARNED it is the logit of a
- * 12 -> 64 -> 64 -> 64 -> 1 ReLU MLP predicting that the winner inserts in its
- * round.  Only the order of insertions changes: the output is the same tet set.
+ * meet only one inserts.  With vote_mode = WTET_VOTE_LEARNED a 12 -> 64 -> 64
+ * -> 64 -> 1 ReLU MLP predicts for each winner that it would insert this
+ * round, and the winner competes with probability min(1, participation/16 *
+ * prediction); the others sit out the round.  Only the order of insertions
+ * changes: the output is the same tet set.
  *
  * Parameters are FP32 in one flat array of WTET_MLP_PARAMS values:
  * W1[64][12] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] W4[64] b4 (row =

@@ -41,7 +41,8 @@ class _Config(ctypes.Structure):
         ("overlap_shift", ctypes.c_uint32),
         ("candidate_filter", ctypes.c_uint32),
         ("pool_factor", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 3),
+        ("participation", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 2),
     ]
 
 
@@ -213,7 +214,7 @@ class Config:
                  enable_splaying: bool = True, max_insert_iterations: int = 100,
                  max_flip_iterations: int = 10, vote: str = "plain", block_size: int = 0,
                  rounds_per_graph: int = 0, overlap_shift: int = 0, candidate_filter: int = 0,
-                 pool_factor: int = 0):
+                 pool_factor: int = 0, participation: int = 0):
         rule = str(insertion_rule).lower()
         if rule not in _RULES:
             raise ValueError(
@@ -234,6 +235,7 @@ class Config:
         self.overlap_shift = int(overlap_shift)
         self.candidate_filter = int(candidate_filter)
         self.pool_factor = int(pool_factor)
+        self.participation = int(participation)
 
     def _c(self) -> _Config:
         if self.vote == "learned":
@@ -252,6 +254,7 @@ class Config:
         c.overlap_shift = self.overlap_shift
         c.candidate_filter = self.candidate_filter
         c.pool_factor = self.pool_factor
+        c.participation = self.participation
         return c
 
     def __repr__(self) -> str:
@@ -372,7 +375,7 @@ def delaunay_batched(clouds, config: Config | None = None):
     stats = st.as_dict()
     for c in range(nc):
         a, b = int(toff[c]), int(toff[c + 1])
-        out.append(DelaunayResult(tets[a:b].copy(), adj[a:b].copy(), np.zeros(0, np.uint32), stats))
+        out.append(DelaunayResult(tets[a:b], adj[a:b], np.zeros(0, np.uint32), stats))
     return out
 
 

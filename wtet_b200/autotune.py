@@ -46,7 +46,7 @@ BUCKETS = (
     (0, 1 << 23, ("mixture", 4_000_000)),
     (0, (1 << 64) - 1, ("mixture", 8_000_000)),
     (1, 1 << 22, ("batched", 256)),
-    (1, (1 << 64) - 1, ("batched", 4096)),
+    (1, (1 << 64) - 1, ("batched", 1024)),
 )
 
 

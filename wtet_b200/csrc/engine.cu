@@ -62,6 +62,10 @@ constexpr uint32_t HUGE_SLOTS = 16;
 // only from the next round (this round's partial claims carry its key).
 constexpr uint8_t kPending = 0x80;
 constexpr uint8_t kDup = 0x40;  // exact duplicate of an earlier point: never inserted
+// Learned scheduler: priority value of a winner that sits out this round, and
+// the number of vote wins after which a winner always competes.
+constexpr uint16_t kSitOut = 0xFFFF;
+constexpr uint32_t kMaxWait = 3;
 constexpr uint32_t WALK_LIMIT = 1u << 22;
 constexpr int ROT_LIMIT = 1 << 16;
 constexpr int kMaxLevels = 15;
@@ -142,9 +146,7 @@ struct Dev {
   uint32_t nv;  // vertices (range guard)
   // clouds
   uint32_t* centry;  // a live tet of each cloud
-  // lists
-  uint32_t* active;
-  uint32_t* active_next;
+  // lists (act / freed above are the double-buffered ones)
   uint32_t* cand;
   uint32_t* cand_off;  // pool offset, or BIG flag | big slot
   uint32_t* cand_len;
@@ -159,8 +161,6 @@ struct Dev {
   uint32_t* pool;
   uint32_t pool_cap;
   uint32_t* big;
-  uint32_t* freed_prev;
-  uint32_t* freed_next;
   Counters* ctr;
   int rule;
   // learned scheduler (vote_mode 1) and its training log (vote_mode 2)
@@ -169,6 +169,7 @@ struct Dev {
   uint8_t* losses;          // vote wins of each point that did not insert
   const mlp::Image* mlp;    // inference weights
   uint16_t* prio;           // claim priority of each vote winner (learned scheduler; null = 0)
+  float participation;      // learned scheduler: competition probability scale
   float* log_x;             // logged features (log_cap x 12)
   uint8_t* log_y;           // logged labels: the winner inserted this round
   uint32_t* log_slot;       // log record of each start, NONE if not sampled
@@ -177,6 +178,11 @@ struct Dev {
 };
 
 struct RoundArgs {
+  // the current lists (the State's parity picks which buffer is which)
+  uint32_t* active;
+  uint32_t* active_next;
+  uint32_t* freed_prev;
+  uint32_t* freed_next;
   unsigned long long stamp;  // (~round mod 2^16) << 48
   uint32_t round;
   uint32_t n_active;
@@ -185,9 +191,11 @@ struct RoundArgs {
   bool live;
 };
 
-// Reads this round's arguments from the device state and points the list
-// fields of D at the current buffers.
-__device__ __forceinline__ RoundArgs load_round(Dev& D) {
+// Reads this round's arguments from the device state, with the current list
+// buffers.  D is not modified and its address never escapes into an
+// out-of-line call, so the kernel parameter block is read in place rather
+// than copied into each thread's local memory.
+__device__ __forceinline__ RoundArgs load_round(const Dev& D) {
   volatile State* S = D.st;
   RoundArgs R;
   R.live = !S->done && !S->stop;
@@ -197,10 +205,10 @@ __device__ __forceinline__ RoundArgs load_round(Dev& D) {
   R.n_freed_prev = S->n_freed_prev;
   R.tet_top = S->tet_top;
   const uint32_t par = S->par & 1u;
-  D.active = D.act[par];
-  D.active_next = D.act[par ^ 1u];
-  D.freed_prev = D.freed[par];
-  D.freed_next = D.freed[par ^ 1u];
+  R.active = par ? D.act[1] : D.act[0];
+  R.active_next = par ? D.act[0] : D.act[1];
+  R.freed_prev = par ? D.freed[1] : D.freed[0];
+  R.freed_next = par ? D.freed[0] : D.freed[1];
   return R;
 }
 
@@ -230,11 +238,14 @@ __device__ __forceinline__ uint32_t mix32(uint32_t h) {
   return h;
 }
 // Claim key of candidate p: round stamp (16 bits, decreasing so that a new
-// round's keys beat every stale one), priority (16 bits, 0 = best; the
-// learned scheduler's, else 0) and a bijective hash of p that breaks ties and
-// identifies the owner.  Smaller keys win.
+// round's keys beat every stale one), priority (16 bits, smaller first) and a
+// bijective hash of p that breaks ties and identifies the owner.  Smaller
+// keys win.  Huge-cavity candidates (bigflag 2, at most HUGE_SLOTS a round)
+// take priority 0: their cavities overlap many others, and at equal priority
+// they would wait until their whole neighbourhood is quiet.  Every other
+// candidate has priority 1 (or kSitOut, set by the learned scheduler).
 __device__ __forceinline__ unsigned long long make_key(const Dev& D, const RoundArgs& R, uint32_t p) {
-  const unsigned long long prio = D.prio ? D.prio[p] : 0u;
+  const unsigned long long prio = D.bigflag[p] == 2 ? 0u : (D.prio ? D.prio[p] : 1u);
   return R.stamp | (prio << 32) | mix32(p ^ (R.round * 0x9E3779B9u));
 }
 
@@ -260,7 +271,8 @@ __device__ __forceinline__ int o3d_sos(const double* a, const double* b, const d
                                        uint32_t* err) {
   int s = ex::orient3d(a, b, c, d, err);
   if (s != 0) return s < 0 ? 1 : -1;
-  return ex::orient3d_sos_degenerate(a, b, c, d, sos[va], sos[vb], sos[vc], sos[vd]);
+  double A[3] = {a[0], a[1], a[2]}, B[3] = {b[0], b[1], b[2]}, C[3] = {c[0], c[1], c[2]}, Dd[3] = {d[0], d[1], d[2]};
+  return ex::orient3d_sos_degenerate(A, B, C, Dd, sos[va], sos[vb], sos[vc], sos[vd]);
 }
 
 __device__ __forceinline__ int o4d_sos(const double* a, const double* b, const double* c, const double* d,
@@ -268,11 +280,13 @@ __device__ __forceinline__ int o4d_sos(const double* a, const double* b, const d
                                        uint32_t ve, const uint32_t* sos, uint32_t* err) {
   int s = ex::insphere(a, b, c, d, e, err);
   if (s != 0) return s;
-  return ex::orient4d_sos_degenerate(a, b, c, d, e, sos[va], sos[vb], sos[vc], sos[vd], sos[ve], err);
+  double A[3] = {a[0], a[1], a[2]}, B[3] = {b[0], b[1], b[2]}, C[3] = {c[0], c[1], c[2]}, Dd[3] = {d[0], d[1], d[2]};
+  double E[3] = {e[0], e[1], e[2]};
+  return ex::orient4d_sos_degenerate(A, B, C, Dd, E, sos[va], sos[vb], sos[vc], sos[vd], sos[ve], err);
 }
 
 // Visibility walk with exact orient3d + SoS from tet t to the tet containing p.
-__device__ uint32_t walk_to(const Dev& D, uint32_t t, uint32_t p, const double* pp, uint32_t& steps) {
+__device__ __forceinline__ uint32_t walk_to(const Dev& D, uint32_t t, uint32_t p, const double* pp, uint32_t& steps) {
   int entry = -1;
   for (uint32_t s = 0; s < WALK_LIMIT; ++s) {
     if (t >= D.cap) {
@@ -545,7 +559,7 @@ __global__ void k_activate(Dev D) {
     uint32_t stride = 1u << level;
     uint32_t pos = (level == C.top) ? k * stride : (2u * k + 1u) * stride;
     uint32_t p = C.vbase + pos;
-    D.active[base + idx] = p;
+    R.active[base + idx] = p;
     if (D.bigflag[p] & kDup) continue;  // never located, dropped by k_relocate
     uint32_t t = NONE;
     if (level < C.top) {
@@ -596,7 +610,7 @@ __global__ void k_vote(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < R.n_active; i += gridDim.x * blockDim.x) {
-    uint32_t p = D.active[i];
+    uint32_t p = R.active[i];
     if (D.bigflag[p] & kDup) continue;
     uint32_t t = D.loc[p];
     if (t >= D.cap) {
@@ -624,7 +638,7 @@ __global__ void k_tcount(Dev D) {
     const uint32_t i = i0 + threadIdx.x;
     uint32_t t = NONE;
     if (i < R.n_active) {
-      const uint32_t p = D.active[i];
+      const uint32_t p = R.active[i];
       if (!(D.bigflag[p] & kDup) && D.loc[p] < D.cap) t = D.loc[p];
     }
     const unsigned peers = __match_any_sync(0xFFFFFFFFu, t);
@@ -659,14 +673,17 @@ __device__ __forceinline__ void winner_features(const Dev& D, const RoundArgs& R
 }
 
 // Learned scheduler, after k_cands: the fused tensor-core MLP scores the
-// vote winners (32 per warp, consecutive in the start list), and each winner
-// draws its claim priority as an exponential clock whose rate is the
-// predicted probability w = sigmoid(score) that it inserts: E = -ln(u) / w
-// with u uniform from a hash, smallest E first (weighted random priorities,
-// Efraimidis & Spirakis 2006).  Likely winners go first more often, while the
-// randomness keeps conflict chains short -- a deterministic score order
-// would let insertions advance only as a front through crowded regions.
-// Then the neighbourhood pre-claim of k_cands is made with those keys.
+// vote winners (32 per warp, consecutive in the start list) with the
+// predicted probability w = sigmoid(score) that each would insert this round,
+// and a winner competes with probability min(1, participation * w); the
+// others sit out the round (no pre-claim, no cavity search).  This is Luby's
+// rule for parallel independent sets -- a vertex joins with a probability
+// that falls with its number of rivals -- with the rival structure learned
+// from the plain method's logs: crowded winners, which would mostly lose and
+// block their neighbours, compete less often, so fewer cavity searches are
+// wasted.  Competitors keep random claim priorities (priority 1), which keeps
+// conflict chains short, and a winner that has sat out or lost kMaxWait times
+// always competes, so nobody starves.
 __global__ void __launch_bounds__(128) k_prio(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
@@ -699,9 +716,10 @@ __global__ void __launch_bounds__(128) k_prio(Dev D) {
       sc = (sc == sc) ? fminf(fmaxf(sc, -20.f), 20.f) : -20.f;
       const uint32_t h = mix32(p * 0x9E3779B1u ^ (R.round * 0x85EBCA6Bu + 0x165667B1u));
       const float u = (float(h >> 8) + 0.5f) * (1.f / 16777216.f);
-      const float clock = -__logf(u) * (1.f + __expf(-sc));  // -ln(u) / sigmoid(sc)
-      D.prio[p] = uint16_t(min(f2o(clock) >> 16, 0xFFFFu));
-      if (D.prefilter) {
+      const float pw = D.participation / (1.f + __expf(-sc));
+      const bool take = D.losses[p] > kMaxWait || u < pw;
+      D.prio[p] = take ? uint16_t(1) : kSitOut;
+      if (take && D.prefilter) {
         const unsigned long long key = make_key(D, R, p);
         atomicMin(&D.pre[t], key);
         const uint4 N = D.tn[t];
@@ -765,54 +783,6 @@ __device__ __forceinline__ bool this_round(const RoundArgs& R, unsigned long lon
   return (key >> 48) == (R.stamp >> 48);
 }
 
-// Grows the cavity of p (tets whose circumsphere holds p, src/phase2.rs:428-470)
-// from its containing tet t0, claiming each cavity tet by atomicMin of the
-// round's key.  Returns K > 0, 0 when a better candidate owns part of the
-// cavity, -1 when the cavity exceeds cap.
-__device__ int grow_cavity(const Dev& D, uint32_t p, const double* pp, uint32_t t0, unsigned long long key,
-                           uint32_t* cav, uint32_t cap) {
-  unsigned long long old = atomicMin(&D.ccav[t0], key);
-  if (old < key) return 0;
-  cav[0] = t0;
-  uint32_t K = 1;
-  for (uint32_t i = 0; i < K; ++i) {
-    uint32_t c = cav[i];
-    uint4 N = D.tn[c];
-    for (int f = 0; f < 4; ++f) {
-      uint32_t nb = comp(N, f);
-      if (nb == NONE) continue;
-      uint32_t nt = nb >> 2;
-      if (nt >= D.cap) {
-        atomicOr(&D.ctr->err, kErrGuard);
-        return 0;
-      }
-      if (__ldcg(&D.ccav[nt]) == key) continue;
-      if (__ldcg(&D.cring[nt]) == key) continue;  // already found outside
-      uint4 W = D.tv[nt];
-      if (W.x >= D.nv || W.y >= D.nv || W.z >= D.nv || W.w >= D.nv) {
-        atomicOr(&D.ctr->err, kErrGuard);
-        return 0;
-      }
-      double P[4][3];
-      load_pt(D.pts, W.x, P[0]);
-      load_pt(D.pts, W.y, P[1]);
-      load_pt(D.pts, W.z, P[2]);
-      load_pt(D.pts, W.w, P[3]);
-      int s = o4d_sos(P[0], P[1], P[2], P[3], pp, W.x, W.y, W.z, W.w, p, D.sos, &D.ctr->err);
-      if (s < 0) {
-        old = atomicMin(&D.ccav[nt], key);
-        if (old < key) return 0;
-        if (old == key) continue;
-        if (K >= cap) return -1;
-        cav[K++] = nt;
-      } else {
-        D.cring[nt] = key;  // memo for this candidate only
-      }
-    }
-  }
-  return int(K);
-}
-
 // Candidates: the vote winner of each tet.  Points whose cavity outgrew the
 // warp scratch in an earlier round go to the huge-cavity path.
 __global__ void k_cands(Dev D) {
@@ -823,7 +793,7 @@ __global__ void k_cands(Dev D) {
     bool start = false;
     uint32_t p = 0;
     if (i < R.n_active) {
-      p = D.active[i];
+      p = R.active[i];
       const uint8_t tier = D.bigflag[p];
       const uint32_t t = D.loc[p];
       if (!(tier & kDup) && t < D.cap && uint32_t(D.vote[t]) == ~p) {
@@ -858,7 +828,7 @@ __global__ void k_cands(Dev D) {
 // tets at once, so the dependent-load chain of a cavity is its BFS depth, not
 // its size.  The cavity is built in the warp's scratch region, then copied to
 // the pool and registered as a candidate.
-__global__ void __launch_bounds__(128) k_bfs(Dev D) {
+__global__ void __launch_bounds__(128, 4) k_bfs(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
   const uint32_t lane = threadIdx.x & 31;
@@ -868,6 +838,7 @@ __global__ void __launch_bounds__(128) k_bfs(Dev D) {
   WARP_LOOP(si, nstart) {
     const uint32_t p = D.starts[si];
     const uint32_t t0 = D.loc[p];
+    if (D.prio && D.prio[p] == kSitOut) continue;  // sits out this round
     const unsigned long long key = make_key(D, R, p);
     double pp[3];
     load_pt(D.pts, p, pp);
@@ -1150,8 +1121,21 @@ __global__ void k_shared(Dev D) {
   }
 }
 
+// The edge of face f of tet V opposite corner k (k != f): its two vertex ids,
+// smaller and larger (register selects, no indexed local array).
+__device__ __forceinline__ uint32_t edge_lo(const uint4& V, int f, int k) {
+  const int q0 = (f != 0 && k != 0) ? 0 : (f != 1 && k != 1) ? 1 : 2;
+  const int q1 = (f != 3 && k != 3) ? 3 : (f != 2 && k != 2) ? 2 : 1;
+  return min(comp(V, q0), comp(V, q1));
+}
+__device__ __forceinline__ uint32_t edge_hi(const uint4& V, int f, int k) {
+  const int q0 = (f != 0 && k != 0) ? 0 : (f != 1 && k != 1) ? 1 : 2;
+  const int q1 = (f != 3 && k != 3) ? 3 : (f != 2 && k != 2) ? 2 : 1;
+  return max(comp(V, q0), comp(V, q1));
+}
+
 __device__ __forceinline__ uint32_t slot_of(const Dev& D, const RoundArgs& R, uint32_t v) {
-  return v < R.n_freed_prev ? D.freed_prev[v] : R.tet_top + (v - R.n_freed_prev);
+  return v < R.n_freed_prev ? R.freed_prev[v] : R.tet_top + (v - R.n_freed_prev);
 }
 
 __device__ __forceinline__ bool boundary_face(const Dev& D, uint32_t nb, unsigned long long key) {
@@ -1218,7 +1202,7 @@ __device__ __forceinline__ uint32_t edge_hash(uint32_t a, uint32_t b) {
   return mix32(a * 0x9E3779B9u ^ b) & (kEdgeSlots - 1);
 }
 
-__global__ void __launch_bounds__(128) k_write(Dev D) {
+__global__ void __launch_bounds__(128, 4) k_write(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
   __shared__ unsigned long long ekey[4][kEdgeSlots];
@@ -1257,11 +1241,7 @@ __global__ void __launch_bounds__(128) k_write(Dev D) {
         {
           for (int k = 0; k < 4; ++k) {
             if (k == f) continue;
-            uint32_t e[2];
-            int ne = 0;
-            for (int q = 0; q < 4; ++q)
-              if (q != f && q != k) e[ne++] = comp(V, q);
-            const uint32_t a = min(e[0], e[1]), b = max(e[0], e[1]);
+            const uint32_t a = edge_lo(V, f, k), b = edge_hi(V, f, k);
             const unsigned long long ek = (static_cast<unsigned long long>(a) << 32) | b;
             const uint32_t val = (sl << 2) | uint32_t(k);
             uint32_t h = edge_hash(a, b);
@@ -1309,11 +1289,7 @@ __global__ void __launch_bounds__(128) k_write(Dev D) {
           if (k == f) continue;
           uint32_t link = NONE;
           if (use_table) {
-            uint32_t e[2];
-            int ne = 0;
-            for (int q = 0; q < 4; ++q)
-              if (q != f && q != k) e[ne++] = comp(V, q);
-            const uint32_t a = min(e[0], e[1]), b = max(e[0], e[1]);
+            const uint32_t a = edge_lo(V, f, k), b = edge_hi(V, f, k);
             const unsigned long long ek = (static_cast<unsigned long long>(a) << 32) | b;
             const uint32_t mine = (sl << 2) | uint32_t(k);
             uint32_t h = edge_hash(a, b);
@@ -1378,7 +1354,7 @@ __global__ void __launch_bounds__(128) k_write(Dev D) {
       uint4 S = D.nslot[c];
       uint32_t fwd = S.x != NONE ? S.x : S.y != NONE ? S.y : S.z != NONE ? S.z : S.w != NONE ? S.w : s0;
       D.tv[c] = make_uint4(DEAD, fwd, 0u, 0u);
-      D.freed_next[fbase + i] = c;
+      R.freed_next[fbase + i] = c;
     }
     if (lane == 0) {
       D.vtet[p] = s0;
@@ -1402,10 +1378,10 @@ __global__ void k_relocate(Dev D) {
     uint32_t i = i0 + threadIdx.x;
     bool keep = false;
     uint32_t p = 0;
-    if (i < R.n_active && (D.bigflag[D.active[i]] & kDup)) {
+    if (i < R.n_active && (D.bigflag[R.active[i]] & kDup)) {
       // exact duplicate: leaves the list without being inserted
     } else if (i < R.n_active) {
-      p = D.active[i];
+      p = R.active[i];
       uint32_t L = D.loc[p];
       uint32_t t = L & ~INS_BIT;
       if (t >= D.cap) {
@@ -1427,7 +1403,7 @@ __global__ void k_relocate(Dev D) {
       }
     }
     uint32_t slot = warp_append(&D.ctr->n_next, keep);
-    if (keep) D.active_next[slot] = p;
+    if (keep) R.active_next[slot] = p;
   }
   if (steps) atomicAdd(&D.ctr->walk_steps, (unsigned long long)steps);
 }
@@ -1481,7 +1457,7 @@ __global__ void k_carry(Dev D) {
   if (R.n_freed_prev <= used) return;
   const uint32_t left = R.n_freed_prev - used;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < left; i += gridDim.x * blockDim.x)
-    D.freed_next[nfn + i] = D.freed_prev[used + i];
+    R.freed_next[nfn + i] = R.freed_prev[used + i];
 }
 
 // End of a round: advance the slot top, swap the lists, stop on errors.
@@ -2140,11 +2116,11 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     D.pts = W.pts.p; D.sos = W.sos.p; D.vcloud = W.vcloud.p; D.vtet = W.vtet.p; D.loc = W.loc.p;
     D.bigflag = W.bigflag.p; D.tv = W.tv.p; D.tn = W.tn.p; D.ccav = W.ccav.p; D.cring = W.cring.p;
     D.nslot = W.nslot.p; D.vote = W.vote.p; D.cap = uint32_t(cap); D.nv = uint32_t(nv); D.centry = W.centry.p;
-    D.active = W.active.p; D.active_next = W.active_next.p; D.cand = W.cand.p; D.cand_off = W.cand_off.p;
+    D.cand = W.cand.p; D.cand_off = W.cand_off.p;
     D.cand_len = W.cand_len.p; D.cand_base = W.cand_base.p; D.st1 = W.st1.p; D.st2 = W.st2.p; D.bigcand = W.bigcand.p;
     D.starts = W.starts.p; D.wscratch = W.wscratch.p; D.pre = W.pre.p;
     D.prefilter = cfg.candidate_filter == 2 ? 0u : 1u; D.pool = W.pool.p; D.pool_cap = pool_cap; D.big = W.big.p;
-    D.freed_prev = W.freed_a.p; D.freed_next = W.freed_b.p; D.ctr = W.ctr.p;
+    D.ctr = W.ctr.p;
     D.st = W.state.p; D.act[0] = W.active.p; D.act[1] = W.active_next.p;
     D.freed[0] = W.freed_a.p; D.freed[1] = W.freed_b.p; D.ci = W.ci.p; D.lvl_off = W.lvl_off.p;
     D.lvl_total = W.lvl_total.p; D.nc = nc;
@@ -2154,6 +2130,7 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     D.losses = vmode ? W.losses.p : nullptr;
     D.mlp = mlp_w;
     D.prio = vmode == 1 ? W.prio.p : nullptr;
+    D.participation = (cfg.participation ? float(cfg.participation) : 40.f) / 16.f;
     D.log_x = job.d_log_x;
     D.log_y = job.d_log_y;
     D.log_slot = vmode == 2 ? W.log_slot.p : nullptr;
@@ -2211,9 +2188,6 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
       uint64_t(std::max<uint32_t>(job.cfg.max_insert_iterations, 1u)) * (maxtop + 1), 65000ull));
   const char* tr = getenv("WTET_TRACE");
   const int trace = tr ? atoi(tr) : 0;
-  cudaEvent_t tev[12];
-  if (trace >= 3)
-    for (auto& e : tev) cudaEventCreate(&e);
   const uint32_t TB = (cfg.block_size == 128 || cfg.block_size == 512) ? cfg.block_size : 256u;
 
   // ---- the round loop, driven from device state and replayed from a graph ----
@@ -2266,17 +2240,29 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   };
   build_graph();
   State hs{};
+  cudaEvent_t tr0 = nullptr, tr1 = nullptr;  // per-round device time when tracing
+  if (trace) {
+    ck(cudaEventCreate(&tr0), "event");
+    ck(cudaEventCreate(&tr1), "event");
+  }
   for (;;) {
+    if (trace) ck(cudaEventRecord(tr0, s), "event record");
     ck(cudaGraphLaunch(gexec, s), "graph launch");
+    if (trace) ck(cudaEventRecord(tr1, s), "event record");
     launches += uint64_t(rpg) * (13 + (vmode == 1 ? 2 : vmode == 2 ? 3 : 0));
     ck(cudaMemcpyAsync(&hs, W.state.p, sizeof(State), cudaMemcpyDeviceToHost, s), "d2h");
     ck(cudaMemcpyAsync(W.h_ctr, W.ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, s), "d2h");
     ck(cudaStreamSynchronize(s), "rounds");
     const Counters& h = *W.h_ctr;
-    if (trace)
-      fprintf(stderr, "[wtet] round %u active %u expanded %llu cand %u inserted %u big %llu alloc %u freed %u top %u err %x\n",
-              hs.round, hs.n_active, (unsigned long long)h.n_expanded, h.n_cand, h.n_inserted,
-              (unsigned long long)h.n_big, h.alloc_used, h.n_freed_next, hs.tet_top, h.err);
+    if (trace) {
+      float rms = 0.f;
+      cudaEventElapsedTime(&rms, tr0, tr1);
+      fprintf(stderr,
+              "[wtet] round %u active %u winners %u expanded %llu cand %u inserted %u big %llu alloc %u top %u "
+              "err %x ms %.3f\n",
+              hs.round, hs.n_active, h.big_used, (unsigned long long)h.n_expanded, h.n_cand, h.n_inserted,
+              (unsigned long long)h.n_big, h.alloc_used, hs.tet_top, h.err, rms);
+    }
     if (hs.stop == 1) {
       if (gexec) cudaGraphExecDestroy(gexec);
       char buf[160];
@@ -2324,6 +2310,8 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     if (hs.done) break;
   }
   if (gexec) cudaGraphExecDestroy(gexec);
+  if (tr0) cudaEventDestroy(tr0);
+  if (tr1) cudaEventDestroy(tr1);
   const uint32_t tet_top = hs.tet_top;
   const uint32_t round = hs.round;
   st.strata = hs.strata;

@@ -294,7 +294,11 @@ __device__ __forceinline__ int orient3d(const double* pa, const double* pb, cons
   double err = kO3dBoundA * perm;
   if (det > err) return 1;
   if (-det > err) return -1;
-  return orient3d_exact_sign(pa, pb, pc, pd, flags);
+  // Fresh copies for the out-of-line exact stage: the caller's coordinate
+  // arrays never have their address taken, so they stay in registers.
+  double a[3] = {pa[0], pa[1], pa[2]}, b[3] = {pb[0], pb[1], pb[2]};
+  double c[3] = {pc[0], pc[1], pc[2]}, d[3] = {pd[0], pd[1], pd[2]};
+  return orient3d_exact_sign(a, b, c, d, flags);
 }
 
 // Sign of Shewchuk insphere(a,b,c,d,e): FP64 filter, then exact.
@@ -327,7 +331,10 @@ __device__ __forceinline__ int insphere(const double* pa, const double* pb, cons
   double err = kIspBoundA * perm;
   if (det > err) return 1;
   if (-det > err) return -1;
-  return insphere_exact_sign(pa, pb, pc, pd, pe, flags);
+  double a[3] = {pa[0], pa[1], pa[2]}, b[3] = {pb[0], pb[1], pb[2]};
+  double c[3] = {pc[0], pc[1], pc[2]}, d[3] = {pd[0], pd[1], pd[2]};
+  double e[3] = {pe[0], pe[1], pe[2]};
+  return insphere_exact_sign(a, b, c, d, e, flags);
 }
 
 // ---- SoS cascade pieces (src/predicates.rs) ----

@@ -1,19 +1,19 @@
 // Learned insertion scheduler: per vote-winner features and the fused BF16
-// MLP that turns them into the winner's insertion priority.
+// MLP that predicts whether a winner would insert in its round.
 //
 // The reference orders insertions by the circumsphere determinant alone
 // (src/shaders/vote.wgsl:401-494); it has no learned scheduler.  Here every
 // tet still votes for the point deepest in its circumsphere, and the winners
 // then compete for their cavities: where two cavities (or their
-// neighbourhoods) meet, the better claim priority inserts this round and the
-// other retries.  The plain method draws that priority at random; the learned
-// scheduler uses the logit of a small MLP (12 -> 64 -> 64 -> 64 -> 1, ReLU,
-// BF16 weights and activations, FP32 accumulate) trained to predict that a
-// winner inserts in its round.  Ranking likely winners first (few rivals,
-// uncrowded neighbourhood) packs more non-conflicting insertions into each
-// round.  Only the order changes: every round still inserts an exactly
-// Delaunay-compatible set of points, so the final tet set is the same unique
-// SoS triangulation.
+// neighbourhoods) meet, one inserts this round and the other retries, so in
+// crowded regions most cavity searches are wasted.  The learned scheduler
+// scores each winner with a small MLP (12 -> 64 -> 64 -> 64 -> 1, ReLU, BF16
+// weights and activations, FP32 accumulate) trained on the plain method's
+// own logs to predict that the winner inserts, and lets it compete only with
+// a probability that grows with that prediction (Luby's rule for parallel
+// independent sets, with the rival structure learned).  Only the order
+// changes: every round still inserts an exactly Delaunay-compatible set of
+// points, so the final tet set is the same unique SoS triangulation.
 //
 // Inference runs on the tensor cores with warp-level mma.m16n8k16 (BF16 in,
 // FP32 accumulate): each warp scores 32 winners at a time, the activations

@@ -2,14 +2,15 @@
 
 Every tet votes for its uninserted point deepest inside its circumsphere (the
 reference's vote, src/shaders/vote.wgsl:401-494); the winners then compete
-for their cavities, and where cavities or their neighbourhoods meet, the
-better claim priority inserts first.  The plain method draws that priority at
-random.  ``Config(vote="learned")`` replaces it by the logit of a small MLP
-(12 -> 64 -> 64 -> 64 -> 1, ReLU) that predicts whether a winner will insert
-in its round, so that likely winners (few rivals, uncrowded neighbourhood)
-go first and each round packs more insertions.  Inference is fused into the
-kernel that resolves the vote (BF16 tensor-core mma, FP32 accumulate); the
-triangulation is unchanged, only the order of insertions.
+for their cavities, and where cavities or their neighbourhoods meet only one
+inserts -- in crowded regions most cavity searches are wasted.
+``Config(vote="learned")`` scores every winner with a small MLP (12 -> 64 ->
+64 -> 64 -> 1, ReLU) that predicts whether it would insert in its round, and
+lets it compete with probability min(1, participation/16 * prediction)
+(Luby's rule for parallel independent sets, with the rival structure learned
+from the plain method's own runs); the rest sit out the round.  Inference is
+fused into the kernel that resolves the vote (BF16 tensor-core mma, FP32
+accumulate); the triangulation is unchanged, only the order of insertions.
 
 Everything here runs on the GPU through libwtet.so:
 
