@@ -99,18 +99,20 @@ struct Counters {
 
 // Round-loop state kept on the device, so that a round is a fixed kernel
 // sequence that can be replayed from a CUDA graph without host round trips.
-struct State {
+struct alignas(16) State {
+  // read by every round kernel: the first 32 bytes, two vector loads
   uint32_t round;         // rounds executed
   uint32_t n_active;      // uninserted points in the current list
   uint32_t par;           // buffer parity: act[par] / freed[par] are current
   uint32_t n_freed_prev;  // recyclable slots in freed[par]
   uint32_t tet_top;       // first never-used tet slot
+  uint32_t done;          // all points inserted
+  uint32_t stop;          // 1 device error, 2 capacity exhausted, 3 no convergence
+  uint32_t pad0;
   int32_t next_level;     // next stratum to locate (-1: none left)
   uint32_t stratum_size;  // size of the last located stratum
   uint32_t strata;
   uint32_t act_level, act_total, act_base;  // stratum located this round
-  uint32_t done;          // all points inserted
-  uint32_t stop;          // 1 device error, 2 capacity exhausted, 3 no convergence
   uint32_t max_rounds;
   uint32_t overlap_shift;
   uint32_t carry_used, carry_left;
@@ -151,6 +153,7 @@ struct Dev {
   uint32_t* cand_off;  // pool offset, or BIG flag | big slot
   uint32_t* cand_len;
   uint32_t* cand_base;
+  uint32_t* cand_nf;   // boundary faces of each winning candidate (k_alloc)
   uint8_t* st1;  // candidate owns its whole cavity
   uint8_t* st2;  // ... and no shared face with a better winner is violated
   uint32_t* bigcand;  // points taking the huge-cavity path this round
@@ -158,6 +161,9 @@ struct Dev {
   unsigned long long* pre;  // neighbourhood pre-claims of the candidates
   uint32_t prefilter;
   uint32_t* wscratch; // one BIG_CAP cavity buffer per warp of k_bfs
+  unsigned long long* etab_key;  // k_write's global edge tables, kEdgeSlotsG per warp
+  uint32_t* etab_val;            // two values per slot
+  uint32_t etab_warps;
   uint32_t* pool;
   uint32_t pool_cap;
   uint32_t* big;
@@ -196,15 +202,18 @@ struct RoundArgs {
 // out-of-line call, so the kernel parameter block is read in place rather
 // than copied into each thread's local memory.
 __device__ __forceinline__ RoundArgs load_round(const Dev& D) {
-  volatile State* S = D.st;
+  // The state was written by earlier kernels of the sequence; kernel
+  // boundaries make it visible, and no round kernel modifies these fields.
+  const uint4 h0 = __ldcg(reinterpret_cast<const uint4*>(D.st));
+  const uint4 h1 = __ldcg(reinterpret_cast<const uint4*>(D.st) + 1);
   RoundArgs R;
-  R.live = !S->done && !S->stop;
-  R.round = S->round;
+  R.live = !h1.y && !h1.z;  // !done && !stop
+  R.round = h0.x;
   R.stamp = (unsigned long long)((~R.round) & 0xFFFFu) << 48;
-  R.n_active = R.live ? S->n_active : 0u;
-  R.n_freed_prev = S->n_freed_prev;
-  R.tet_top = S->tet_top;
-  const uint32_t par = S->par & 1u;
+  R.n_active = R.live ? h0.y : 0u;
+  R.n_freed_prev = h0.w;
+  R.tet_top = h1.x;
+  const uint32_t par = h0.z & 1u;
   R.active = par ? D.act[1] : D.act[0];
   R.active_next = par ? D.act[0] : D.act[1];
   R.freed_prev = par ? D.freed[1] : D.freed[0];
@@ -694,7 +703,7 @@ __global__ void __launch_bounds__(128) k_prio(Dev D) {
   mlp::load_image(S, D.mlp);
   __syncthreads();
   const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t nstart = *(volatile uint32_t*)&D.ctr->big_used;
+  const uint32_t nstart = __ldcg(&D.ctr->big_used);
   const uint32_t warps = gridDim.x * (blockDim.x >> 5);
   for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + w) * 32; base < nstart; base += warps * 32) {
     const uint32_t i = base + lane;
@@ -737,7 +746,7 @@ __global__ void __launch_bounds__(128) k_prio(Dev D) {
 __global__ void k_log_features(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
-  const uint32_t nstart = *(volatile uint32_t*)&D.ctr->big_used;
+  const uint32_t nstart = __ldcg(&D.ctr->big_used);
   for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nstart; s += gridDim.x * blockDim.x) {
     const uint32_t p = D.starts[s];
     uint32_t slot = NONE;
@@ -760,7 +769,7 @@ __global__ void k_log_features(Dev D) {
 __global__ void k_log_labels(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
-  const uint32_t nstart = *(volatile uint32_t*)&D.ctr->big_used;
+  const uint32_t nstart = __ldcg(&D.ctr->big_used);
   for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nstart; s += gridDim.x * blockDim.x) {
     const uint32_t slot = D.log_slot[s];
     if (slot != NONE) D.log_y[slot] = (D.loc[D.starts[s]] & INS_BIT) ? 1 : 0;
@@ -833,8 +842,13 @@ __global__ void __launch_bounds__(128, 4) k_bfs(Dev D) {
   if (!R.live) return;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  // BFS queue: the first kBfsShared entries in shared memory, the rest in
+  // the warp's global region (most cavities never leave shared memory).
+  constexpr uint32_t kBfsShared = 256;
+  __shared__ uint32_t sq_all[4][kBfsShared];
+  uint32_t* sq = sq_all[threadIdx.x >> 5];
   uint32_t* cav = D.wscratch + size_t(warp) * BIG_CAP;
-  const uint32_t nstart = *(volatile uint32_t*)&D.ctr->big_used;
+  const uint32_t nstart = __ldcg(&D.ctr->big_used);
   WARP_LOOP(si, nstart) {
     const uint32_t p = D.starts[si];
     const uint32_t t0 = D.loc[p];
@@ -855,7 +869,7 @@ __global__ void __launch_bounds__(128, 4) k_bfs(Dev D) {
     if (lane == 0) {
       unsigned long long old = atomicMin(&D.ccav[t0], key);
       lost = old < key;
-      cav[0] = t0;
+      sq[0] = t0;
     }
     lost = __shfl_sync(0xFFFFFFFFu, lost, 0);
     uint32_t K = 1, head = 0;
@@ -870,7 +884,7 @@ __global__ void __launch_bounds__(128, 4) k_bfs(Dev D) {
       bool add = false, my_lost = false, my_guard = false;
       uint32_t nt = 0;
       if (idx < K) {
-        const uint32_t c = cav[idx];
+        const uint32_t c = idx < kBfsShared ? sq[idx] : cav[idx];
         const uint32_t nb = reinterpret_cast<const uint32_t*>(D.tn + c)[f];
         if (nb != NONE) {
           nt = nb >> 2;
@@ -901,7 +915,8 @@ __global__ void __launch_bounds__(128, 4) k_bfs(Dev D) {
       const unsigned ball = __ballot_sync(0xFFFFFFFFu, add);
       const uint32_t pos = K + __popc(ball & ((1u << lane) - 1u));
       if (add) {
-        if (pos < BIG_CAP) cav[pos] = nt;
+        if (pos < kBfsShared) sq[pos] = nt;
+        else if (pos < BIG_CAP) cav[pos] = nt;
         else overflow = true;
       }
       if (__any_sync(0xFFFFFFFFu, my_guard)) {
@@ -925,7 +940,7 @@ __global__ void __launch_bounds__(128, 4) k_bfs(Dev D) {
     if (lane == 0) off = atomicAdd(&D.ctr->pool_used, K);
     off = __shfl_sync(0xFFFFFFFFu, off, 0);
     if (off + K > D.pool_cap) continue;  // pool full: retry next round
-    for (uint32_t k = lane; k < K; k += 32) D.pool[off + k] = cav[k];
+    for (uint32_t k = lane; k < K; k += 32) D.pool[off + k] = k < kBfsShared ? sq[k] : cav[k];
     if (lane == 0) {
       const uint32_t ci = atomicAdd(&D.ctr->n_cand, 1u);
       D.cand[ci] = p;
@@ -954,7 +969,7 @@ __global__ void k_expand_big(Dev D) {
   if (!R.live) return;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t nbig = 0;  // the warp path of k_bfs covers cavities up to BIG_CAP
-  const uint32_t nhuge = min(*(volatile uint32_t*)&D.ctr->huge_used, HUGE_SLOTS);
+  const uint32_t nhuge = min(__ldcg(&D.ctr->huge_used), HUGE_SLOTS);
   WARP_LOOP(wi, nbig + nhuge) {
     const bool huge = wi >= nbig;
     const uint32_t bi = huge ? BIG_SLOTS + (wi - nbig) : wi;
@@ -1054,7 +1069,7 @@ __global__ void k_resolve(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
   const uint32_t lane = threadIdx.x & 31;
-  const uint32_t ncand = *(volatile uint32_t*)&D.ctr->n_cand;
+  const uint32_t ncand = __ldcg(&D.ctr->n_cand);
   WARP_LOOP(ci, ncand) {
     uint32_t p = D.cand[ci];
     uint32_t K = D.cand_len[ci];
@@ -1076,7 +1091,7 @@ __global__ void k_shared(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
   const uint32_t lane = threadIdx.x & 31;
-  const uint32_t ncand = *(volatile uint32_t*)&D.ctr->n_cand;
+  const uint32_t ncand = __ldcg(&D.ctr->n_cand);
   WARP_LOOP(ci, ncand) {
     uint32_t p = D.cand[ci];
     if (!D.st1[p]) {
@@ -1147,7 +1162,7 @@ __global__ void k_alloc(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
   const uint32_t lane = threadIdx.x & 31;
-  const uint32_t ncand = *(volatile uint32_t*)&D.ctr->n_cand;
+  const uint32_t ncand = __ldcg(&D.ctr->n_cand);
   WARP_LOOP(ci, ncand) {
     uint32_t p = D.cand[ci];
     if (!D.st2[p]) continue;
@@ -1185,21 +1200,28 @@ __global__ void k_alloc(Dev D) {
         if (boundary_face(D, comp(N, f), key)) set_comp(S, f, slot_of(D, R, j++));
       D.nslot[c] = S;
     }
-    if (lane == 0) D.cand_base[ci] = base;
+    if (lane == 0) {
+      D.cand_base[ci] = base;
+      D.cand_nf[ci] = total;
+    }
   }
 }
 
 // Writes the new tets of every winner.  The three faces through p of a new
-// tet pair up across the boundary edges of the cavity: for cavities of up to
-// kEdgeFaces boundary faces the pairs are matched in a per-warp shared-memory
-// edge table; larger ones rotate around each edge inside the cavity.  A
-// boundary face shared with another winner's cavity links to that winner's
-// new tet.
-constexpr uint32_t kEdgeSlots = 256;  // per warp; load <= 0.47 at kEdgeFaces faces
+// tet pair up across the boundary edges of the cavity (each boundary edge is
+// shared by exactly two new tets): the pairs are matched in an open-addressing
+// edge table of at least 3 slots per boundary face (load <= 1/2) -- in shared
+// memory for up to kEdgeFaces faces, in the warp's region of a global table
+// for up to kEdgeFacesG faces -- and larger cavities rotate around each edge
+// inside the cavity.  A boundary face shared with another winner's cavity
+// links to that winner's new tet.
+constexpr uint32_t kEdgeSlots = 256;    // shared-memory slots per warp
 constexpr uint32_t kEdgeFaces = 80;
+constexpr uint32_t kEdgeSlotsG = 1024;  // global slots per warp
+constexpr uint32_t kEdgeFacesG = 340;
 
-__device__ __forceinline__ uint32_t edge_hash(uint32_t a, uint32_t b) {
-  return mix32(a * 0x9E3779B9u ^ b) & (kEdgeSlots - 1);
+__device__ __forceinline__ uint32_t edge_hash(uint32_t a, uint32_t b, uint32_t mask) {
+  return mix32(a * 0x9E3779B9u ^ b) & mask;
 }
 
 __global__ void __launch_bounds__(128, 4) k_write(Dev D) {
@@ -1209,27 +1231,34 @@ __global__ void __launch_bounds__(128, 4) k_write(Dev D) {
   __shared__ uint32_t ev0[4][kEdgeSlots], ev1[4][kEdgeSlots];
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t w = threadIdx.x >> 5;
-  const uint32_t ncand = *(volatile uint32_t*)&D.ctr->n_cand;
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t ncand = __ldcg(&D.ctr->n_cand);
   WARP_LOOP(ci, ncand) {
     uint32_t p = D.cand[ci];
     if (!D.st2[p]) continue;
     uint32_t K = D.cand_len[ci];
     const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
     unsigned long long key = make_key(D, R, p);
-    // Boundary faces of the cavity (those with a new slot).
-    uint32_t Fl = 0;
-    for (uint32_t i = lane; i < K; i += 32) {
-      const uint4 S = D.nslot[cav[i]];
-      Fl += (S.x != NONE) + (S.y != NONE) + (S.z != NONE) + (S.w != NONE);
+    const uint32_t F = D.cand_nf[ci];  // boundary faces, counted by k_alloc
+    unsigned long long* tk = nullptr;
+    uint32_t *t0 = nullptr, *t1 = nullptr;
+    uint32_t mask = 31;
+    while (mask + 1 < 3 * F) mask = 2 * mask + 1;
+    if (F <= kEdgeFaces) {
+      tk = ekey[w];
+      t0 = ev0[w];
+      t1 = ev1[w];
+    } else if (F <= kEdgeFacesG && gwarp < D.etab_warps) {
+      tk = D.etab_key + size_t(gwarp) * kEdgeSlotsG;
+      t0 = D.etab_val + size_t(gwarp) * 2 * kEdgeSlotsG;
+      t1 = t0 + kEdgeSlotsG;
     }
-    uint32_t F = Fl;
-    for (int o = 16; o > 0; o >>= 1) F += __shfl_xor_sync(0xFFFFFFFFu, F, o);
-    const bool use_table = F <= kEdgeFaces;
+    const bool use_table = tk != nullptr;
     if (use_table) {
-      for (uint32_t j = lane; j < kEdgeSlots; j += 32) {
-        ekey[w][j] = ~0ull;
-        ev0[w][j] = NONE;
-        ev1[w][j] = NONE;
+      for (uint32_t j = lane; j <= mask; j += 32) {
+        tk[j] = ~0ull;
+        t0[j] = NONE;
+        t1[j] = NONE;
       }
       __syncwarp();
       for (uint32_t e = lane; e < 4 * K; e += 32) {
@@ -1244,14 +1273,14 @@ __global__ void __launch_bounds__(128, 4) k_write(Dev D) {
             const uint32_t a = edge_lo(V, f, k), b = edge_hi(V, f, k);
             const unsigned long long ek = (static_cast<unsigned long long>(a) << 32) | b;
             const uint32_t val = (sl << 2) | uint32_t(k);
-            uint32_t h = edge_hash(a, b);
-            for (uint32_t probe = 0; probe < kEdgeSlots; ++probe) {
-              const unsigned long long old = atomicCAS(&ekey[w][h], ~0ull, ek);
+            uint32_t h = edge_hash(a, b, mask);
+            for (uint32_t probe = 0; probe <= mask; ++probe) {
+              const unsigned long long old = atomicCAS(&tk[h], ~0ull, ek);
               if (old == ~0ull || old == ek) {
-                if (atomicCAS(&ev0[w][h], NONE, val) != NONE) ev1[w][h] = val;
+                if (atomicCAS(&t0[h], NONE, val) != NONE) t1[h] = val;
                 break;
               }
-              h = (h + 1) & (kEdgeSlots - 1);
+              h = (h + 1) & mask;
             }
           }
         }
@@ -1292,15 +1321,15 @@ __global__ void __launch_bounds__(128, 4) k_write(Dev D) {
             const uint32_t a = edge_lo(V, f, k), b = edge_hi(V, f, k);
             const unsigned long long ek = (static_cast<unsigned long long>(a) << 32) | b;
             const uint32_t mine = (sl << 2) | uint32_t(k);
-            uint32_t h = edge_hash(a, b);
-            for (uint32_t probe = 0; probe < kEdgeSlots; ++probe) {
-              const unsigned long long kk = ekey[w][h];
+            uint32_t h = edge_hash(a, b, mask);
+            for (uint32_t probe = 0; probe <= mask; ++probe) {
+              const unsigned long long kk = tk[h];
               if (kk == ek) {
-                link = ev0[w][h] == mine ? ev1[w][h] : ev0[w][h];
+                link = t0[h] == mine ? t1[h] : t0[h];
                 break;
               }
               if (kk == ~0ull) break;
-              h = (h + 1) & (kEdgeSlots - 1);
+              h = (h + 1) & mask;
             }
           } else {
             uint32_t cur = c;
@@ -1452,8 +1481,8 @@ __global__ void k_begin(Dev D) {
 __global__ void k_carry(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
-  const uint32_t used = *(volatile uint32_t*)&D.ctr->alloc_used;
-  const uint32_t nfn = *(volatile uint32_t*)&D.ctr->n_freed_next;
+  const uint32_t used = __ldcg(&D.ctr->alloc_used);
+  const uint32_t nfn = __ldcg(&D.ctr->n_freed_next);
   if (R.n_freed_prev <= used) return;
   const uint32_t left = R.n_freed_prev - used;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < left; i += gridDim.x * blockDim.x)
@@ -1750,9 +1779,10 @@ struct Workspace {
   DBuf<uint8_t> bigflag;
   DBuf<uint4> tv, tn, nslot;
   DBuf<unsigned long long> ccav, cring, vote, pre;
-  DBuf<uint32_t> centry, active, active_next, cand, cand_off, cand_len, cand_base, pool, big, freed_a, freed_b;
+  DBuf<uint32_t> centry, active, active_next, cand, cand_off, cand_len, cand_base, cand_nf, pool, big, freed_a, freed_b;
   DBuf<uint8_t> st1, st2;
-  DBuf<uint32_t> bigcand, starts, wscratch;
+  DBuf<uint32_t> bigcand, starts, wscratch, etab_val;
+  DBuf<unsigned long long> etab_key;
   DBuf<uint64_t> lvl_off;
   DBuf<uint32_t> lvl_total;
   DBuf<State> state;
@@ -1796,6 +1826,16 @@ Workspace& ws() {
   return *tl_ws;
 }
 
+// One full wave of resident blocks of kernel k on the current device.
+template <class K>
+uint32_t wave(K* k, uint32_t threads) {
+  int dev = 0, sms = 0, per = 0;
+  ck(cudaGetDevice(&dev), "cudaGetDevice");
+  ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "device attribute");
+  ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, int(threads), 0), "occupancy");
+  return uint32_t(std::max(1, per) * std::max(1, sms));
+}
+
 inline uint32_t blocks_for(uint64_t n, uint32_t threads, uint32_t cap = 148 * 16) {
   uint64_t b = (n + threads - 1) / threads;
   if (b < 1) b = 1;
@@ -1828,10 +1868,11 @@ void release_thread_workspace() {
   w.vcloud.release(); w.vtet.release(); w.loc.release(); w.bigflag.release(); w.tv.release();
   w.tn.release(); w.nslot.release(); w.ccav.release(); w.cring.release(); w.pre.release(); w.vote.release();
   w.centry.release(); w.active.release(); w.active_next.release(); w.cand.release();
-  w.cand_off.release(); w.cand_len.release(); w.cand_base.release(); w.st1.release(); w.st2.release(); w.bigcand.release(); w.starts.release(); w.wscratch.release(); w.pool.release(); w.big.release();
+  w.cand_off.release(); w.cand_len.release(); w.cand_base.release(); w.cand_nf.release(); w.st1.release(); w.st2.release(); w.bigcand.release(); w.starts.release(); w.wscratch.release(); w.pool.release(); w.big.release();
   w.freed_a.release(); w.freed_b.release(); w.lvl_off.release(); w.lvl_total.release(); w.state.release(); w.ctr.release();
   w.ccount.release(); w.hullcnt.release(); w.cfill.release(); w.newid.release();
   w.hull.release(); w.coff.release(); w.out_t.release(); w.out_a.release(); w.dtab.release(); w.dup.release();
+  w.etab_key.release(); w.etab_val.release();
   w.tcount.release(); w.log_slot.release(); w.losses.release(); w.prio.release();
   for (auto& b : w.scan_tmp) b.release();
   if (w.h_ctr) cudaFreeHost(w.h_ctr);
@@ -2055,10 +2096,14 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   W.cand_off.reserve(n, "cand");
   W.cand_len.reserve(n, "cand");
   W.cand_base.reserve(n, "cand");
+  W.cand_nf.reserve(n, "cand");
   W.st1.reserve(nv, "status");
   W.bigcand.reserve(BIG_SLOTS + HUGE_SLOTS, "bigcand");
   W.starts.reserve(n, "starts");
-  W.wscratch.reserve(size_t(148) * 16 * 4 * BIG_CAP, "warp scratch");
+  W.wscratch.reserve(size_t(wave(k_bfs, 128)) * 4 * BIG_CAP, "warp scratch");  // one queue per warp of a k_bfs wave
+  const uint32_t etab_warps = wave(k_write, 128) * 4;  // one edge table per warp of a k_write wave
+  W.etab_key.reserve(size_t(etab_warps) * kEdgeSlotsG, "edge tables");
+  W.etab_val.reserve(size_t(etab_warps) * 2 * kEdgeSlotsG, "edge tables");
   W.st2.reserve(nv, "status");
   const uint64_t pool_factor = std::min<uint32_t>(std::max<uint32_t>(cfg.pool_factor, 4u), 64u);
   const uint32_t pool_cap = uint32_t(std::min<uint64_t>(std::max<uint64_t>(n * pool_factor, 1 << 16), 1ull << 30));
@@ -2117,8 +2162,9 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     D.bigflag = W.bigflag.p; D.tv = W.tv.p; D.tn = W.tn.p; D.ccav = W.ccav.p; D.cring = W.cring.p;
     D.nslot = W.nslot.p; D.vote = W.vote.p; D.cap = uint32_t(cap); D.nv = uint32_t(nv); D.centry = W.centry.p;
     D.cand = W.cand.p; D.cand_off = W.cand_off.p;
-    D.cand_len = W.cand_len.p; D.cand_base = W.cand_base.p; D.st1 = W.st1.p; D.st2 = W.st2.p; D.bigcand = W.bigcand.p;
+    D.cand_len = W.cand_len.p; D.cand_base = W.cand_base.p; D.cand_nf = W.cand_nf.p; D.st1 = W.st1.p; D.st2 = W.st2.p; D.bigcand = W.bigcand.p;
     D.starts = W.starts.p; D.wscratch = W.wscratch.p; D.pre = W.pre.p;
+    D.etab_key = W.etab_key.p; D.etab_val = W.etab_val.p; D.etab_warps = etab_warps;
     D.prefilter = cfg.candidate_filter == 2 ? 0u : 1u; D.pool = W.pool.p; D.pool_cap = pool_cap; D.big = W.big.p;
     D.ctr = W.ctr.p;
     D.st = W.state.p; D.act[0] = W.active.p; D.act[1] = W.active_next.p;
@@ -2202,25 +2248,31 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   ck(cudaMemcpyAsync(W.state.p, &S0, sizeof(State), cudaMemcpyHostToDevice, s), "h2d");
   ck(cudaMemsetAsync(W.ctr.p, 0, sizeof(Counters), s), "memset");
 
-  const uint32_t GT = 148 * 8;         // thread kernels: 256-thread blocks, grid-stride
-  const uint32_t GW = 148 * 16;        // warp-per-candidate kernels: 128-thread blocks
+  // Every round kernel loops grid-stride over its work, so each gets exactly
+  // one full wave of resident blocks: an idle round then costs one short
+  // wave per kernel.
   const uint32_t GB = (BIG_SLOTS + HUGE_SLOTS) / 4;
+  const uint32_t g_act = wave(k_activate, TB), g_tc = wave(k_tcount, TB), g_vote = wave(k_vote, TB);
+  const uint32_t g_cand = wave(k_cands, TB), g_prio = wave(k_prio, 128), g_logf = wave(k_log_features, TB);
+  const uint32_t g_bfs = wave(k_bfs, 128), g_res = wave(k_resolve, 128), g_sh = wave(k_shared, 128);
+  const uint32_t g_al = wave(k_alloc, 128), g_wr = wave(k_write, 128), g_rel = wave(k_relocate, TB);
+  const uint32_t g_logl = wave(k_log_labels, TB);
   auto enqueue_round = [&]() {
     k_begin<<<1, 32, 0, s>>>(D);
-    k_activate<<<GT, TB, 0, s>>>(D);
-    if (vmode) k_tcount<<<GT, TB, 0, s>>>(D);
-    k_vote<<<GT, TB, 0, s>>>(D);
-    k_cands<<<GT, TB, 0, s>>>(D);
-    if (vmode == 1) k_prio<<<148 * 4, 128, 0, s>>>(D);
-    if (vmode == 2) k_log_features<<<GT, TB, 0, s>>>(D);
-    k_bfs<<<GW, 128, 0, s>>>(D);
+    k_activate<<<g_act, TB, 0, s>>>(D);
+    if (vmode) k_tcount<<<g_tc, TB, 0, s>>>(D);
+    k_vote<<<g_vote, TB, 0, s>>>(D);
+    k_cands<<<g_cand, TB, 0, s>>>(D);
+    if (vmode == 1) k_prio<<<g_prio, 128, 0, s>>>(D);
+    if (vmode == 2) k_log_features<<<g_logf, TB, 0, s>>>(D);
+    k_bfs<<<g_bfs, 128, 0, s>>>(D);
     k_expand_big<<<GB, 128, 0, s>>>(D);
-    k_resolve<<<GW, 128, 0, s>>>(D);
-    k_shared<<<GW, 128, 0, s>>>(D);
-    k_alloc<<<GW, 128, 0, s>>>(D);
-    k_write<<<GW, 128, 0, s>>>(D);
-    k_relocate<<<GT, TB, 0, s>>>(D);
-    if (vmode == 2) k_log_labels<<<GT, TB, 0, s>>>(D);
+    k_resolve<<<g_res, 128, 0, s>>>(D);
+    k_shared<<<g_sh, 128, 0, s>>>(D);
+    k_alloc<<<g_al, 128, 0, s>>>(D);
+    k_write<<<g_wr, 128, 0, s>>>(D);
+    k_relocate<<<g_rel, TB, 0, s>>>(D);
+    if (vmode == 2) k_log_labels<<<g_logl, TB, 0, s>>>(D);
     k_carry<<<148, TB, 0, s>>>(D);
     k_end<<<1, 32, 0, s>>>(D);
   };
