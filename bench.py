@@ -356,10 +356,9 @@ WORKLOADS = {
 
 
 def _canon_digest(tets):
-    import hashlib
+    from wtet_b200.autotune import tet_set_digest
 
-    t = np.sort(np.asarray(tets, np.int64), axis=1)
-    return hashlib.sha256(t[np.lexsort(t.T[::-1])].tobytes()).hexdigest()
+    return tet_set_digest(tets)
 
 
 def variants(wt, args):

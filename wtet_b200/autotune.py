@@ -118,12 +118,21 @@ def _workload(spec, seed=7):
     return syn.batched_clouds(size, seed)
 
 
+def tet_set_digest(tets) -> str:
+    """Order-independent digest of a tet set: each tet's sorted vertex ids
+    are mixed into a 64-bit value and the values summed (mod 2^64), so no
+    sort of the whole set is needed."""
+    t = np.sort(np.asarray(tets).astype(np.uint64), axis=1)
+    h = t[:, 0] * np.uint64(0x9E3779B97F4A7C15)
+    for k, c in ((1, 0xBF58476D1CE4E5B9), (2, 0x94D049BB133111EB), (3, 0xD6E8FEB86659FD93)):
+        h = (h ^ (h >> np.uint64(29))) * np.uint64(c) + t[:, k]
+    h = h ^ (h >> np.uint64(32))
+    return f"{int(h.sum(dtype=np.uint64)):016x}:{t.shape[0]}"
+
+
 def _digest(results) -> str:
-    h = hashlib.sha256()
-    for r in results:
-        t = np.sort(r.tets.astype(np.int64), axis=1)
-        h.update(t[np.lexsort(t.T[::-1])].tobytes())
-    return h.hexdigest()
+    return "|".join(tet_set_digest(r.tets) for r in results) if len(results) < 8 else \
+        tet_set_digest(np.concatenate([r.tets for r in results]))
 
 
 def _measure(clouds, knobs, repeats):

@@ -160,7 +160,7 @@ struct Dev {
   uint32_t* starts;   // vote winners expanding their cavity this round
   unsigned long long* pre;  // neighbourhood pre-claims of the candidates
   uint32_t prefilter;
-  uint32_t* wscratch; // one BIG_CAP cavity buffer per warp of k_bfs
+  uint32_t* wscratch; // one BIG_CAP cavity queue per lane group of k_bfs
   unsigned long long* etab_key;  // k_write's global edge tables, kEdgeSlotsG per warp
   uint32_t* etab_val;            // two values per slot
   uint32_t etab_warps;
@@ -833,57 +833,75 @@ __global__ void k_cands(Dev D) {
   }
 }
 
-// Warp-cooperative cavity growth: the 32 lanes test the faces of 32 frontier
-// tets at once, so the dependent-load chain of a cavity is its BFS depth, not
-// its size.  The cavity is built in the warp's scratch region, then copied to
-// the pool and registered as a candidate.
+// Cavity growth by groups of kBfsLanes lanes, kWarpGroups candidates per
+// warp: a group tests kBfsLanes (queued tet, face) pairs per pass, so a small
+// cavity costs one dependent load chain (tet -> neighbour -> claim ->
+// vertices -> coordinates -> insphere -> claim) per pass, and a warp keeps
+// several such chains in flight.  The queue starts in shared memory and
+// continues in the group's global region; cavities beyond BIG_CAP move to the
+// huge path next round.
+constexpr uint32_t kBfsLanes = 16;
+constexpr uint32_t kWarpGroups = 32 / kBfsLanes;
+constexpr uint32_t kBfsShared = 128;  // queue entries per group in shared memory
+
 __global__ void __launch_bounds__(128, 4) k_bfs(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
-  const uint32_t lane = threadIdx.x & 31;
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  // BFS queue: the first kBfsShared entries in shared memory, the rest in
-  // the warp's global region (most cavities never leave shared memory).
-  constexpr uint32_t kBfsShared = 256;
-  __shared__ uint32_t sq_all[4][kBfsShared];
-  uint32_t* sq = sq_all[threadIdx.x >> 5];
-  uint32_t* cav = D.wscratch + size_t(warp) * BIG_CAP;
+  constexpr uint32_t FULL = 0xFFFFFFFFu, GM = (kBfsLanes == 32) ? 0xFFFFFFFFu : ((1u << kBfsLanes) - 1u);
+  __shared__ uint32_t sq_all[4 * kWarpGroups][kBfsShared];
+  const uint32_t lane = threadIdx.x & 31, gl = lane % kBfsLanes, shift = lane - gl;
+  const uint32_t lt = (1u << gl) - 1u;
+  const uint32_t gid = (blockIdx.x * blockDim.x + threadIdx.x) / kBfsLanes;  // global group index
+  const uint32_t ngroups = gridDim.x * blockDim.x / kBfsLanes;
+  uint32_t* sq = sq_all[threadIdx.x / kBfsLanes];
+  uint32_t* cav = D.wscratch + size_t(gid) * BIG_CAP;
   const uint32_t nstart = __ldcg(&D.ctr->big_used);
-  WARP_LOOP(si, nstart) {
-    const uint32_t p = D.starts[si];
-    const uint32_t t0 = D.loc[p];
-    if (D.prio && D.prio[p] == kSitOut) continue;  // sits out this round
-    const unsigned long long key = make_key(D, R, p);
-    double pp[3];
-    load_pt(D.pts, p, pp);
-    int lost = 0;
-    if (D.prefilter && lane < 5) {
+  const uint32_t first = gid - gid % kWarpGroups;  // the warp's first group: warp-uniform loop bounds
+  for (uint32_t base = first; base < nstart; base += ngroups) {
+    const uint32_t si = base + gid % kWarpGroups;
+    bool active = si < nstart;
+    uint32_t p = 0, t0 = 0;
+    if (active) {
+      p = D.starts[si];
+      t0 = D.loc[p];
+      if (D.prio && D.prio[p] == kSitOut) active = false;  // sits out this round
+    }
+    unsigned long long key = 0;
+    double pp[3] = {0.0, 0.0, 0.0};
+    if (active) {
+      key = make_key(D, R, p);
+      load_pt(D.pts, p, pp);
+    }
+    int pre_lost = 0;
+    if (active && D.prefilter && gl < 5) {
       uint32_t t = t0;
-      if (lane > 0) {
-        const uint32_t nb = comp(D.tn[t0], lane - 1);
+      if (gl > 0) {
+        const uint32_t nb = comp(D.tn[t0], gl - 1);
         t = nb == NONE ? NONE : nb >> 2;
       }
-      if (t != NONE && t < D.cap && __ldcg(&D.pre[t]) != key) lost = 1;
+      if (t != NONE && t < D.cap && __ldcg(&D.pre[t]) != key) pre_lost = 1;
     }
-    if (__any_sync(0xFFFFFFFFu, lost)) continue;
-    if (lane == 0) {
-      unsigned long long old = atomicMin(&D.ccav[t0], key);
-      lost = old < key;
+    // warp collectives first, outside any short-circuit: every lane must reach them
+    const uint32_t g_pre = (__ballot_sync(FULL, pre_lost) >> shift) & GM;
+    const bool searched = active && !g_pre;
+    int claim_lost = 0;
+    if (searched && gl == 0) {
+      const unsigned long long old = atomicMin(&D.ccav[t0], key);
+      claim_lost = old < key;
       sq[0] = t0;
     }
-    lost = __shfl_sync(0xFFFFFFFFu, lost, 0);
+    const int g_claim = __shfl_sync(FULL, claim_lost, shift);
+    bool lost = !searched || g_claim;
     uint32_t K = 1, head = 0;
     bool overflow = false;
+    bool running = !lost;
     __syncwarp();
-    // Each pass tests 32 (frontier tet, face) pairs, one per lane: 8 queued
-    // tets x 4 faces, so a small frontier costs one dependent load chain per
-    // pass instead of one per face.
-    while (!lost && !overflow && head < K) {
-      const uint32_t idx = head + (lane >> 2);
-      const uint32_t f = lane & 3u;
+    while (__any_sync(FULL, running)) {
       bool add = false, my_lost = false, my_guard = false;
       uint32_t nt = 0;
-      if (idx < K) {
+      const uint32_t idx = head + gl / 4u;
+      const uint32_t f = gl & 3u;
+      if (running && idx < K) {
         const uint32_t c = idx < kBfsShared ? sq[idx] : cav[idx];
         const uint32_t nb = reinterpret_cast<const uint32_t*>(D.tn + c)[f];
         if (nb != NONE) {
@@ -912,40 +930,46 @@ __global__ void __launch_bounds__(128, 4) k_bfs(Dev D) {
           }
         }
       }
-      const unsigned ball = __ballot_sync(0xFFFFFFFFu, add);
-      const uint32_t pos = K + __popc(ball & ((1u << lane) - 1u));
+      const uint32_t gball = (__ballot_sync(FULL, add) >> shift) & GM;
+      const uint32_t pos = K + __popc(gball & lt);
+      bool my_over = false;
       if (add) {
         if (pos < kBfsShared) sq[pos] = nt;
         else if (pos < BIG_CAP) cav[pos] = nt;
-        else overflow = true;
+        else my_over = true;
       }
-      if (__any_sync(0xFFFFFFFFu, my_guard)) {
-        if (lane == 0) atomicOr(&D.ctr->err, kErrGuard);
-        lost = 1;
+      const bool g_guard = (__ballot_sync(FULL, my_guard) >> shift) & GM;
+      const bool g_lost = (__ballot_sync(FULL, my_lost) >> shift) & GM;
+      const bool g_over = (__ballot_sync(FULL, my_over) >> shift) & GM;
+      if (running) {
+        if (g_guard) {
+          if (gl == 0) atomicOr(&D.ctr->err, kErrGuard);
+          lost = true;
+        }
+        lost = lost || g_lost;
+        overflow = overflow || g_over;
+        head = min(head + kBfsLanes / 4u, K);
+        K += __popc(gball);
+        running = !lost && !overflow && head < K;
       }
-      lost |= __any_sync(0xFFFFFFFFu, my_lost);
-      overflow = __any_sync(0xFFFFFFFFu, overflow);
-      head = min(head + 8u, K);
-      K += __popc(ball);
       __syncwarp();
     }
-    if (lane == 0) atomicAdd(&D.ctr->n_expanded, 1ull);
-    if (overflow) {
-      // Partial claims carry this round's key: the huge path takes it next round.
-      if (lane == 0) D.bigflag[p] = kPending | 2;
-      continue;
-    }
-    if (lost) continue;
+    if (searched && gl == 0) atomicAdd(&D.ctr->n_expanded, 1ull);
+    // Partial claims carry this round's key: the huge path takes it next round.
+    if (searched && overflow && gl == 0) D.bigflag[p] = kPending | 2;
+    bool ok = searched && !lost && !overflow;
     uint32_t off = 0;
-    if (lane == 0) off = atomicAdd(&D.ctr->pool_used, K);
-    off = __shfl_sync(0xFFFFFFFFu, off, 0);
-    if (off + K > D.pool_cap) continue;  // pool full: retry next round
-    for (uint32_t k = lane; k < K; k += 32) D.pool[off + k] = k < kBfsShared ? sq[k] : cav[k];
-    if (lane == 0) {
-      const uint32_t ci = atomicAdd(&D.ctr->n_cand, 1u);
-      D.cand[ci] = p;
-      D.cand_off[ci] = off;
-      D.cand_len[ci] = K;
+    if (ok && gl == 0) off = atomicAdd(&D.ctr->pool_used, K);
+    off = __shfl_sync(FULL, off, shift);
+    ok = ok && off + K <= D.pool_cap;  // pool full: retry next round
+    if (ok) {
+      for (uint32_t k = gl; k < K; k += kBfsLanes) D.pool[off + k] = k < kBfsShared ? sq[k] : cav[k];
+      if (gl == 0) {
+        const uint32_t ci = atomicAdd(&D.ctr->n_cand, 1u);
+        D.cand[ci] = p;
+        D.cand_off[ci] = off;
+        D.cand_len[ci] = K;
+      }
     }
     __syncwarp();
   }
@@ -2100,7 +2124,8 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   W.st1.reserve(nv, "status");
   W.bigcand.reserve(BIG_SLOTS + HUGE_SLOTS, "bigcand");
   W.starts.reserve(n, "starts");
-  W.wscratch.reserve(size_t(wave(k_bfs, 128)) * 4 * BIG_CAP, "warp scratch");  // one queue per warp of a k_bfs wave
+  // one overflow queue per lane group of a k_bfs wave
+  W.wscratch.reserve(size_t(wave(k_bfs, 128)) * (128 / kBfsLanes) * BIG_CAP, "cavity queues");
   const uint32_t etab_warps = wave(k_write, 128) * 4;  // one edge table per warp of a k_write wave
   W.etab_key.reserve(size_t(etab_warps) * kEdgeSlotsG, "edge tables");
   W.etab_val.reserve(size_t(etab_warps) * 2 * kEdgeSlotsG, "edge tables");
