@@ -319,8 +319,10 @@ def run_gpu(args):
             "unit": "GB/s",
             "frac": round(achieved / hbm, 5),
             "traffic": TRAFFIC.get(args.workload),
-            "basis": "whole triangulation per step: 12 B/point read + 32 B/tet written over its device time; "
-                     f"peak = {peak_kind} copy bandwidth",
+            "basis": "whole triangulation per step (about 3,000 launches of 13 round kernels replayed from CUDA "
+                     "graphs, so no single launch is the unit): 12 B/point read + 32 B/tet written over its "
+                     f"device time; peak = {peak_kind} copy bandwidth; traffic = DRAM bytes of one "
+                     "triangulation from ncu (1M mixture, scaled by points)",
         },
         "clocks": clocks.summary(),
     }
@@ -336,9 +338,17 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
-# DRAM bytes (read + write) per triangulation measured with ncu on a 1M-point
-# case of the same distribution and scaled by the point count (profiles/).
-TRAFFIC: dict = {}
+# DRAM bytes (read + write) per triangulation, from an ncu launch list of one
+# triangulation of the 1M-point mixture (dram__bytes_read.sum +
+# dram__bytes_write.sum over all launches, --cache-control none), scaled by the
+# point count for the larger clouds of the same distribution
+# (profiles/launch_list_mixture1M.md).
+_TRAFFIC_1M_MIXTURE = 37.434e9
+TRAFFIC: dict = {
+    "mixture1M": _TRAFFIC_1M_MIXTURE,
+    "mixture8M": 8 * _TRAFFIC_1M_MIXTURE,
+    "mixture8M_new": 8 * _TRAFFIC_1M_MIXTURE,
+}
 
 WORKLOADS = {
     "mixture8M": "8,000,000 points: 60% uniform [0,1]^3, 30% Gaussian ball (0.5, sigma 0.1), "
