@@ -72,8 +72,7 @@ def make_workload(name: str, rank: int = 0, world: int = 1):
     if name == "uniform100k":
         return [syn.uniform(100_000, 1)]
     if name == "batched":
-        clouds = syn.batched_clouds(4096, 4)
-        return clouds[rank::world]
+        return shard(syn.batched_clouds(4096, 4), rank, world)
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -131,7 +130,9 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_setup(n_gpus):
+def dist_setup(n_gpus, backend: str = "nccl"):
+    """One process per GPU (torchrun env); a short process-group timeout so
+    that ranks waiting on a dead peer end with an error."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -140,19 +141,32 @@ def dist_setup(n_gpus):
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return rank, local, world
 
 
-def max_over_ranks(x: float, world: int) -> float:
+def reduce_over_ranks(x: float, world: int, op: str = "max", device: str = "cuda") -> float:
+    """max / sum of a scalar over all ranks (the same value on every rank)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    return reduce_over_ranks(x, world, "max")
+
+
+def shard(clouds, rank: int, world: int):
+    """Clouds of a batched workload owned by one rank (round robin); a
+    single cloud is not split -- every rank runs a replica."""
+    if len(clouds) == 1:
+        return clouds
+    return clouds[rank::world]
 
 
 def barrier(world):
@@ -242,11 +256,7 @@ def run_gpu(args):
     ms_step = elapsed_ms / args.steps
     total_points = n_points * (world if len(clouds) == 1 else 1)
     if len(clouds) > 1 and world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([n_points], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t)
-        total_points = int(t.item())
+        total_points = int(reduce_over_ranks(float(n_points), world, "sum"))
     value = total_points / (ms_step * 1e3)
 
     # ---- end-to-end arm: C ABI from pinned host buffers, copies inside ----
