@@ -52,12 +52,12 @@ namespace wtet {
 constexpr uint32_t NONE = 0xFFFFFFFFu;
 constexpr uint32_t DEAD = 0xFFFFFFFFu;  // tv.x of a retired tet; tv.y then forwards to a live tet
 constexpr uint32_t INS_BIT = 0x80000000u;
-// Cavity tiers: one warp with up to BIG_CAP tets in its scratch region, then
-// one warp with up to HUGE_CAP tets in a global slot.
-constexpr uint32_t BIG_CAP = 1u << 12;
-constexpr uint32_t BIG_SLOTS = 1024;   // large cavities expanded per round
+// Cavity tiers: a lane group of k_bfs grows cavities of up to BIG_CAP tets;
+// larger ones are re-grown the next round by a whole block (k_expand_big) in
+// one of HUGE_SLOTS global slots of up to HUGE_CAP tets, with claim priority 0.
+constexpr uint32_t BIG_CAP = 512;
 constexpr uint32_t HUGE_CAP = 1u << 18;
-constexpr uint32_t HUGE_SLOTS = 16;
+constexpr uint32_t HUGE_SLOTS = 64;
 // bigflag: tier (0 warp scratch, 2 huge slot) | kPending while the tier applies
 // only from the next round (this round's partial claims carry its key).
 constexpr uint8_t kPending = 0x80;
@@ -90,6 +90,7 @@ struct Counters {
   uint32_t big_used;      // large-cavity slots used
   uint32_t n_inserted;    // winners this round
   uint32_t huge_used;     // huge-cavity slots used
+  uint32_t btab_used;     // k_write's large edge tables handed out this round
   uint32_t err;           // error flags
   unsigned long long walk_steps;
   unsigned long long n_expanded;
@@ -164,6 +165,8 @@ struct Dev {
   unsigned long long* etab_key;  // k_write's global edge tables, kEdgeSlotsG per warp
   uint32_t* etab_val;            // two values per slot
   uint32_t etab_warps;
+  unsigned long long* btab_key;  // kBigTables tables of kBigTableSlots for larger cavities
+  uint32_t* btab_val;
   uint32_t* pool;
   uint32_t pool_cap;
   uint32_t* big;
@@ -809,7 +812,7 @@ __global__ void k_cands(Dev D) {
         if (D.losses && D.losses[p] < 255u) D.losses[p] += 1u;
         if (tier == 2) {
           uint32_t b = atomicAdd(&D.ctr->huge_used, 1u);
-          if (b < HUGE_SLOTS) D.bigcand[BIG_SLOTS + b] = p;
+          if (b < HUGE_SLOTS) D.bigcand[b] = p;
         } else if (!tier) {
           start = true;
           D.st1[p] = 0;
@@ -975,10 +978,9 @@ __global__ void __launch_bounds__(128, 4) k_bfs(Dev D) {
   }
 }
 
-// Global cavity slot bi: BIG_SLOTS slots of BIG_CAP, then HUGE_SLOTS of HUGE_CAP.
+// Global cavity slot bi of the huge path (HUGE_CAP tets each).
 __device__ __forceinline__ uint32_t* big_slot(const Dev& D, uint32_t bi) {
-  return bi < BIG_SLOTS ? D.big + size_t(bi) * BIG_CAP
-                        : D.big + size_t(BIG_SLOTS) * BIG_CAP + size_t(bi - BIG_SLOTS) * HUGE_CAP;
+  return D.big + size_t(bi) * HUGE_CAP;
 }
 
 __device__ __forceinline__ const uint32_t* cand_cavity(const Dev& D, uint32_t off) {
@@ -986,104 +988,91 @@ __device__ __forceinline__ const uint32_t* cand_cavity(const Dev& D, uint32_t of
 }
 
 
-// Large cavities: one warp per point; the cavity list doubles as the BFS
-// queue and is grown 32 tets at a time.
-__global__ void k_expand_big(Dev D) {
+// Huge cavities: one block per candidate; each pass tests blockDim/4 queued
+// tets x 4 faces, appending to the slot's list through a shared counter.
+__global__ void __launch_bounds__(256) k_expand_big(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
-  const uint32_t lane = threadIdx.x & 31;
-  const uint32_t nbig = 0;  // the warp path of k_bfs covers cavities up to BIG_CAP
   const uint32_t nhuge = min(__ldcg(&D.ctr->huge_used), HUGE_SLOTS);
-  WARP_LOOP(wi, nbig + nhuge) {
-    const bool huge = wi >= nbig;
-    const uint32_t bi = huge ? BIG_SLOTS + (wi - nbig) : wi;
-    const uint32_t cap = huge ? HUGE_CAP : BIG_CAP;
-    uint32_t p = D.bigcand[bi];
-    uint32_t t0 = D.loc[p];
-    uint32_t* cav = big_slot(D, bi);
-    unsigned long long key = make_key(D, R, p);
-    double pp[3];
-    load_pt(D.pts, p, pp);
-    int lost = 0;
-    if (lane == 0) {
-      D.st1[p] = 0;
-      D.st2[p] = 0;
-      unsigned long long old = atomicMin(&D.ccav[t0], key);
-      lost = old < key;
-      cav[0] = t0;
-    }
-    lost = __shfl_sync(0xFFFFFFFFu, lost, 0);
-    uint32_t K = 1, head = 0;
-    bool overflow = false;
-    __syncwarp();
-    while (!lost && !overflow && head < K) {
-      uint32_t idx = head + lane;
-      bool valid = idx < K;
-      uint32_t c = valid ? cav[idx] : 0u;
-      uint4 N = valid ? D.tn[c] : make_uint4(NONE, NONE, NONE, NONE);
-      uint32_t newK = K;
-      bool my_lost = false, my_guard = false;
-      for (int f = 0; f < 4; ++f) {
-        bool add = false;
-        uint32_t nt = 0;
-        uint32_t nb = comp(N, f);
-        if (valid && nb != NONE) {
-          nt = nb >> 2;
-          if (nt >= D.cap) {
-            my_guard = true;
-          } else if (__ldcg(&D.ccav[nt]) != key && __ldcg(&D.cring[nt]) != key) {
-            uint4 W = D.tv[nt];
-            if (W.x >= D.nv || W.y >= D.nv || W.z >= D.nv || W.w >= D.nv) {
-              my_guard = true;
-            } else {
-              double P[4][3];
-              load_pt(D.pts, W.x, P[0]);
-              load_pt(D.pts, W.y, P[1]);
-              load_pt(D.pts, W.z, P[2]);
-              load_pt(D.pts, W.w, P[3]);
-              int sg = o4d_sos(P[0], P[1], P[2], P[3], pp, W.x, W.y, W.z, W.w, p, D.sos, &D.ctr->err);
-              if (sg < 0) {
-                unsigned long long old = atomicMin(&D.ccav[nt], key);
-                if (old < key) my_lost = true;
-                else if (old != key) add = true;
-              } else {
-                D.cring[nt] = key;
+  const uint32_t bi = blockIdx.x;
+  if (bi >= nhuge) return;  // block-uniform
+  __shared__ uint32_t sK, sNew, sHead, sLost, sOver, sGuard;
+  const uint32_t tid = threadIdx.x;
+  const uint32_t p = D.bigcand[bi];
+  const uint32_t t0 = D.loc[p];
+  uint32_t* cav = big_slot(D, bi);
+  const unsigned long long key = make_key(D, R, p);
+  double pp[3];
+  load_pt(D.pts, p, pp);
+  if (tid == 0) {
+    D.st1[p] = 0;
+    D.st2[p] = 0;
+    const unsigned long long old = t0 < D.cap ? atomicMin(&D.ccav[t0], key) : 0ull;
+    sLost = old < key ? 1u : 0u;
+    sOver = 0u;
+    sGuard = t0 < D.cap ? 0u : 1u;
+    cav[0] = t0;
+    sK = 1u;
+    sNew = 1u;
+    sHead = 0u;
+  }
+  __syncthreads();
+  for (;;) {
+    const uint32_t K = sK, head = sHead;
+    const bool stop = sLost || sOver || sGuard || head >= K;
+    __syncthreads();  // every thread has read the pass state
+    if (stop) break;   // block-uniform
+    const uint32_t idx = head + tid / 4u, f = tid & 3u;
+    if (idx < K) {
+      const uint32_t c = cav[idx];
+      const uint32_t nb = reinterpret_cast<const uint32_t*>(D.tn + c)[f];
+      if (nb != NONE) {
+        const uint32_t nt = nb >> 2;
+        if (nt >= D.cap) {
+          sGuard = 1u;
+        } else if (__ldcg(&D.ccav[nt]) != key && __ldcg(&D.cring[nt]) != key) {
+          const uint4 W = D.tv[nt];
+          if (W.x >= D.nv || W.y >= D.nv || W.z >= D.nv || W.w >= D.nv) {
+            sGuard = 1u;
+          } else {
+            double P[4][3];
+            load_pt(D.pts, W.x, P[0]);
+            load_pt(D.pts, W.y, P[1]);
+            load_pt(D.pts, W.z, P[2]);
+            load_pt(D.pts, W.w, P[3]);
+            const int sg = o4d_sos(P[0], P[1], P[2], P[3], pp, W.x, W.y, W.z, W.w, p, D.sos, &D.ctr->err);
+            if (sg < 0) {
+              const unsigned long long old = atomicMin(&D.ccav[nt], key);
+              if (old < key) {
+                sLost = 1u;
+              } else if (old != key) {
+                const uint32_t pos = atomicAdd(&sNew, 1u);
+                if (pos < HUGE_CAP) cav[pos] = nt;
+                else sOver = 1u;
               }
+            } else {
+              D.cring[nt] = key;
             }
           }
         }
-        unsigned ball = __ballot_sync(0xFFFFFFFFu, add);
-        uint32_t pos = newK + __popc(ball & ((1u << lane) - 1u));
-        if (add) {
-          if (pos < cap) cav[pos] = nt;
-          else overflow = true;
-        }
-        newK += __popc(ball);
       }
-      if (__any_sync(0xFFFFFFFFu, my_guard)) {
-        if (lane == 0) atomicOr(&D.ctr->err, kErrGuard);
-        lost = 1;
-      }
-      lost |= __any_sync(0xFFFFFFFFu, my_lost);
-      overflow = __any_sync(0xFFFFFFFFu, overflow);
-      head = min(head + 32u, K);
-      K = newK;
-      __syncwarp();
     }
-    if (lane == 0) atomicAdd(&D.ctr->n_big, 1ull);
-    if (overflow) {
-      if (lane == 0) {
-        if (huge) atomicOr(&D.ctr->err, kErrBig);
-        else D.bigflag[p] = kPending | 2;
-      }
-      continue;
+    __syncthreads();
+    if (tid == 0) {
+      sHead = min(head + blockDim.x / 4u, K);
+      sK = min(sNew, HUGE_CAP);
     }
-    if (lost) continue;
-    if (lane == 0) {
-      uint32_t ci = atomicAdd(&D.ctr->n_cand, 1u);
+    __syncthreads();
+  }
+  if (tid == 0) {
+    atomicAdd(&D.ctr->n_big, 1ull);
+    if (sGuard) atomicOr(&D.ctr->err, kErrGuard);
+    if (sOver) atomicOr(&D.ctr->err, kErrBig);
+    if (!sLost && !sOver && !sGuard) {
+      const uint32_t ci = atomicAdd(&D.ctr->n_cand, 1u);
       D.cand[ci] = p;
       D.cand_off[ci] = 0x80000000u | bi;
-      D.cand_len[ci] = K;
+      D.cand_len[ci] = sK;
     }
   }
 }
@@ -1236,13 +1225,17 @@ __global__ void k_alloc(Dev D) {
 // shared by exactly two new tets): the pairs are matched in an open-addressing
 // edge table of at least 3 slots per boundary face (load <= 1/2) -- in shared
 // memory for up to kEdgeFaces faces, in the warp's region of a global table
-// for up to kEdgeFacesG faces -- and larger cavities rotate around each edge
-// inside the cavity.  A boundary face shared with another winner's cavity
+// for up to kEdgeFacesG faces, in one of kBigTables large tables (taken per
+// round, first come) for up to kBigTableFaces -- and the rest rotate around
+// each edge inside the cavity.  A boundary face shared with another winner's cavity
 // links to that winner's new tet.
 constexpr uint32_t kEdgeSlots = 256;    // shared-memory slots per warp
 constexpr uint32_t kEdgeFaces = 80;
 constexpr uint32_t kEdgeSlotsG = 1024;  // global slots per warp
 constexpr uint32_t kEdgeFacesG = 340;
+constexpr uint32_t kBigTables = 16;         // large tables per round, taken first come
+constexpr uint32_t kBigTableSlots = 1u << 14;
+constexpr uint32_t kBigTableFaces = kBigTableSlots / 3;
 
 __device__ __forceinline__ uint32_t edge_hash(uint32_t a, uint32_t b, uint32_t mask) {
   return mix32(a * 0x9E3779B9u ^ b) & mask;
@@ -1276,6 +1269,15 @@ __global__ void __launch_bounds__(128, 4) k_write(Dev D) {
       tk = D.etab_key + size_t(gwarp) * kEdgeSlotsG;
       t0 = D.etab_val + size_t(gwarp) * 2 * kEdgeSlotsG;
       t1 = t0 + kEdgeSlotsG;
+    } else if (F <= kBigTableFaces) {
+      uint32_t bt = 0;
+      if (lane == 0) bt = atomicAdd(&D.ctr->btab_used, 1u);
+      bt = __shfl_sync(0xFFFFFFFFu, bt, 0);
+      if (bt < kBigTables) {
+        tk = D.btab_key + size_t(bt) * kBigTableSlots;
+        t0 = D.btab_val + size_t(bt) * 2 * kBigTableSlots;
+        t1 = t0 + kBigTableSlots;
+      }
     }
     const bool use_table = tk != nullptr;
     if (use_table) {
@@ -1499,6 +1501,7 @@ __global__ void k_begin(Dev D) {
   C->big_used = 0;
   C->n_inserted = 0;
   C->huge_used = 0;
+  C->btab_used = 0;
 }
 
 // Recycled slots that were not handed out this round carry over.
@@ -1806,7 +1809,8 @@ struct Workspace {
   DBuf<uint32_t> centry, active, active_next, cand, cand_off, cand_len, cand_base, cand_nf, pool, big, freed_a, freed_b;
   DBuf<uint8_t> st1, st2;
   DBuf<uint32_t> bigcand, starts, wscratch, etab_val;
-  DBuf<unsigned long long> etab_key;
+  DBuf<unsigned long long> etab_key, btab_key;
+  DBuf<uint32_t> btab_val;
   DBuf<uint64_t> lvl_off;
   DBuf<uint32_t> lvl_total;
   DBuf<State> state;
@@ -1896,7 +1900,7 @@ void release_thread_workspace() {
   w.freed_a.release(); w.freed_b.release(); w.lvl_off.release(); w.lvl_total.release(); w.state.release(); w.ctr.release();
   w.ccount.release(); w.hullcnt.release(); w.cfill.release(); w.newid.release();
   w.hull.release(); w.coff.release(); w.out_t.release(); w.out_a.release(); w.dtab.release(); w.dup.release();
-  w.etab_key.release(); w.etab_val.release();
+  w.etab_key.release(); w.etab_val.release(); w.btab_key.release(); w.btab_val.release();
   w.tcount.release(); w.log_slot.release(); w.losses.release(); w.prio.release();
   for (auto& b : w.scan_tmp) b.release();
   if (w.h_ctr) cudaFreeHost(w.h_ctr);
@@ -2122,18 +2126,20 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   W.cand_base.reserve(n, "cand");
   W.cand_nf.reserve(n, "cand");
   W.st1.reserve(nv, "status");
-  W.bigcand.reserve(BIG_SLOTS + HUGE_SLOTS, "bigcand");
+  W.bigcand.reserve(HUGE_SLOTS, "bigcand");
   W.starts.reserve(n, "starts");
   // one overflow queue per lane group of a k_bfs wave
   W.wscratch.reserve(size_t(wave(k_bfs, 128)) * (128 / kBfsLanes) * BIG_CAP, "cavity queues");
   const uint32_t etab_warps = wave(k_write, 128) * 4;  // one edge table per warp of a k_write wave
   W.etab_key.reserve(size_t(etab_warps) * kEdgeSlotsG, "edge tables");
   W.etab_val.reserve(size_t(etab_warps) * 2 * kEdgeSlotsG, "edge tables");
+  W.btab_key.reserve(size_t(kBigTables) * kBigTableSlots, "edge tables");
+  W.btab_val.reserve(size_t(kBigTables) * 2 * kBigTableSlots, "edge tables");
   W.st2.reserve(nv, "status");
   const uint64_t pool_factor = std::min<uint32_t>(std::max<uint32_t>(cfg.pool_factor, 4u), 64u);
   const uint32_t pool_cap = uint32_t(std::min<uint64_t>(std::max<uint64_t>(n * pool_factor, 1 << 16), 1ull << 30));
   W.pool.reserve(pool_cap, "pool");
-  W.big.reserve(size_t(BIG_SLOTS) * BIG_CAP + size_t(HUGE_SLOTS) * HUGE_CAP, "big");
+  W.big.reserve(size_t(HUGE_SLOTS) * HUGE_CAP, "big");
   W.ctr.reserve(1, "counters");
   W.lvl_off.reserve(size_t(maxtop + 1) * (nc + 1), "levels");
   W.lvl_total.reserve(maxtop + 1, "levels");
@@ -2190,6 +2196,7 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     D.cand_len = W.cand_len.p; D.cand_base = W.cand_base.p; D.cand_nf = W.cand_nf.p; D.st1 = W.st1.p; D.st2 = W.st2.p; D.bigcand = W.bigcand.p;
     D.starts = W.starts.p; D.wscratch = W.wscratch.p; D.pre = W.pre.p;
     D.etab_key = W.etab_key.p; D.etab_val = W.etab_val.p; D.etab_warps = etab_warps;
+    D.btab_key = W.btab_key.p; D.btab_val = W.btab_val.p;
     D.prefilter = cfg.candidate_filter == 2 ? 0u : 1u; D.pool = W.pool.p; D.pool_cap = pool_cap; D.big = W.big.p;
     D.ctr = W.ctr.p;
     D.st = W.state.p; D.act[0] = W.active.p; D.act[1] = W.active_next.p;
@@ -2276,7 +2283,7 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   // Every round kernel loops grid-stride over its work, so each gets exactly
   // one full wave of resident blocks: an idle round then costs one short
   // wave per kernel.
-  const uint32_t GB = (BIG_SLOTS + HUGE_SLOTS) / 4;
+  const uint32_t GB = HUGE_SLOTS;  // one block per huge-cavity slot
   const uint32_t g_act = wave(k_activate, TB), g_tc = wave(k_tcount, TB), g_vote = wave(k_vote, TB);
   const uint32_t g_cand = wave(k_cands, TB), g_prio = wave(k_prio, 128), g_logf = wave(k_log_features, TB);
   const uint32_t g_bfs = wave(k_bfs, 128), g_res = wave(k_resolve, 128), g_sh = wave(k_shared, 128);
@@ -2291,7 +2298,7 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     if (vmode == 1) k_prio<<<g_prio, 128, 0, s>>>(D);
     if (vmode == 2) k_log_features<<<g_logf, TB, 0, s>>>(D);
     k_bfs<<<g_bfs, 128, 0, s>>>(D);
-    k_expand_big<<<GB, 128, 0, s>>>(D);
+    k_expand_big<<<GB, 256, 0, s>>>(D);
     k_resolve<<<g_res, 128, 0, s>>>(D);
     k_shared<<<g_sh, 128, 0, s>>>(D);
     k_alloc<<<g_al, 128, 0, s>>>(D);
