@@ -55,8 +55,8 @@ enum wtet_vote_mode { WTET_VOTE_PLAIN = 0, WTET_VOTE_LEARNED = 1 };
 typedef struct wtet_config {
   uint32_t insertion_rule;         /* wtet_insertion_rule, default circumcenter */
   uint32_t enable_flipping;        /* accepted for compatibility; default 1 */
-  uint32_t enable_sorting;         /* accepted; spatial order never changes SoS */
-  uint32_t enable_hilbert_sorting; /* accepted; spatial order never changes SoS */
+  uint32_t enable_sorting;         /* accepted: the device always inserts along a space-filling curve */
+  uint32_t enable_hilbert_sorting; /* 1: insert in Hilbert instead of Morton order (never changes the result) */
   uint32_t enable_splaying;        /* accepted; the device path needs no repair */
   uint32_t max_insert_iterations;  /* cap on insertion rounds per stratum, default 100 */
   uint32_t max_flip_iterations;    /* accepted for compatibility; default 10 */
@@ -246,6 +246,15 @@ int wtet_autotune_set_table(const wtet_tune_entry* entries, uint32_t count);
 int wtet_autotune_get_table(wtet_tune_entry* entries, uint32_t capacity, uint32_t* count);
 /* The knobs a job of n points in num_clouds clouds would run with. */
 int wtet_autotune_resolve(const wtet_config* cfg, uint64_t n, uint32_t num_clouds, wtet_config* out);
+
+/* Cell indices of the point order (host functions, no GPU needed).  Points
+ * are bucketed on a per-cloud grid of up to 2^10 cells per axis and inserted
+ * in Morton order (default) or, with enable_hilbert_sorting, Hilbert order --
+ * the reference's two sorts (src/morton.rs:22-80, src/hilbert.rs:20-38).
+ * Neither changes the triangulation.  wtet_hilbert_index returns 0xFFFFFFFF
+ * for bits outside 1..10. */
+uint32_t wtet_morton_index(uint32_t x, uint32_t y, uint32_t z);
+uint32_t wtet_hilbert_index(uint32_t x, uint32_t y, uint32_t z, uint32_t bits);
 
 /* Upper bound on the output tet count for n points (for sizing buffers). */
 uint64_t wtet_max_tets(uint64_t n);

@@ -150,3 +150,26 @@ def test_full_size_properties(gpu, oracle_mod, name, make):
     assert v == 0 and interior > 2 * n
     if n <= 2_100_000:
         assert euler(fin) == 1
+
+
+def test_full_size_batched(gpu):
+    """The batched configuration at its benchmark size (4,096 clouds of
+    log-uniform sizes in [64, 65536], about 40M points): every cloud's output
+    is structurally valid and passes the device exact local-Delaunay check,
+    and a sample of clouds is identical to triangulating them one by one."""
+    from wtet_b200.autotune import tet_set_digest
+
+    clouds = fx.batched_clouds(4096, 4)
+    res = gpu.delaunay_batched(clouds)
+    assert len(res) == len(clouds)
+    for pts, r in zip(clouds, res):
+        n = len(pts)
+        assert (r.tets == n + 4).any(axis=1).sum() == 4
+        v, interior = gpu.check_quality(pts, r)
+        assert v == 0 and interior > 0
+    rng = np.random.default_rng(7)
+    for i in rng.choice(len(clouds), 48, replace=False):
+        r = res[i]
+        check_adjacency(r.tets, r.adjacency)
+        single = gpu.delaunay(clouds[i])
+        assert tet_set_digest(single.tets) == tet_set_digest(r.tets), i

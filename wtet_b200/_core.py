@@ -100,6 +100,8 @@ EXPORTS = (
     "wtet_autotune_set_table",
     "wtet_autotune_get_table",
     "wtet_autotune_resolve",
+    "wtet_morton_index",
+    "wtet_hilbert_index",
 )
 
 
@@ -176,6 +178,10 @@ def load():
     L.wtet_autotune_get_table.restype = ctypes.c_int
     L.wtet_autotune_resolve.argtypes = [ctypes.POINTER(_Config), u64, ctypes.c_uint32, ctypes.POINTER(_Config)]
     L.wtet_autotune_resolve.restype = ctypes.c_int
+    L.wtet_morton_index.argtypes = [ctypes.c_uint32] * 3
+    L.wtet_morton_index.restype = ctypes.c_uint32
+    L.wtet_hilbert_index.argtypes = [ctypes.c_uint32] * 4
+    L.wtet_hilbert_index.restype = ctypes.c_uint32
     _lib = L
     _install_packaged_table()
     return L

@@ -11,6 +11,7 @@
 
 #include "../../include/wtet.h"
 #include "engine.cuh"
+#include "order.cuh"
 
 namespace {
 
@@ -299,6 +300,16 @@ int wtet_autotune_resolve(const wtet_config* cfg, uint64_t n, uint32_t num_cloud
   if (!out) return fail(WTET_ERR_ARG, "null pointer argument");
   *out = wtet::tuned_config(resolve(cfg), n, num_clouds ? num_clouds : 1u);
   return WTET_OK;
+}
+
+uint32_t wtet_morton_index(uint32_t x, uint32_t y, uint32_t z) {
+  return wtet::morton3(x & 1023u, y & 1023u, z & 1023u);
+}
+
+uint32_t wtet_hilbert_index(uint32_t x, uint32_t y, uint32_t z, uint32_t bits) {
+  if (bits < 1 || bits > 10) return 0xFFFFFFFFu;
+  const uint32_t m = (1u << bits) - 1u;
+  return wtet::hilbert3(x & m, y & m, z & m, bits);
 }
 
 int wtet_initialize_gpu(char* buf, size_t len) { return device_string(buf, len, true); }

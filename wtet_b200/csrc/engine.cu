@@ -46,6 +46,7 @@
 #include "engine.cuh"
 #include "exact.cuh"
 #include "learned.cuh"
+#include "order.cuh"
 
 namespace wtet {
 
@@ -411,19 +412,13 @@ struct CloudInfo {
   uint32_t pad;
 };
 
-__device__ __forceinline__ uint32_t expand10(uint32_t v) {
-  v = (v | (v << 16)) & 0x030000FFu;
-  v = (v | (v << 8)) & 0x0300F00Fu;
-  v = (v | (v << 4)) & 0x030C30C3u;
-  v = (v | (v << 2)) & 0x09249249u;
-  return v;
-}
+
 
 // Normalises (src/lib.rs:325-334, f32 arithmetic) and buckets each point by a
 // per-cloud Morton code; counts bucket sizes.
 __global__ void k_normalize(const float* xyz, const uint64_t* off, const CloudInfo* ci, uint32_t nc, uint64_t n,
                             const uint32_t* mn, const uint32_t* mx, float4* tmp, uint32_t* bucket,
-                            uint32_t* hist) {
+                            uint32_t* hist, int hilbert) {
   uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
   uint32_t c = cloud_of(off, nc, i);
@@ -444,7 +439,7 @@ __global__ void k_normalize(const float* xyz, const uint64_t* off, const CloudIn
     uint32_t u = (v > 0.f) ? (v >= float(res) ? res - 1 : uint32_t(v)) : 0u;
     code[k] = u;
   }
-  uint32_t b = C.bbase + ((expand10(code[2]) << 2) | (expand10(code[1]) << 1) | expand10(code[0]));
+  uint32_t b = C.bbase + (hilbert ? hilbert3(code[0], code[1], code[2], C.bbits) : morton3(code[0], code[1], code[2]));
   bucket[i] = b;
   atomicAdd(&hist[b], 1u);
 }
@@ -2221,7 +2216,8 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   const uint32_t T = 256;
   uint32_t nb = uint32_t((n + T - 1) / T);
   k_bbox<<<nb, T, 0, s>>>(job.d_xyz, W.off.p, nc, n, W.mn.p, W.mx.p);
-  k_normalize<<<nb, T, 0, s>>>(job.d_xyz, W.off.p, W.ci.p, nc, n, W.mn.p, W.mx.p, W.tmp.p, W.bucket.p, W.hist.p);
+  k_normalize<<<nb, T, 0, s>>>(job.d_xyz, W.off.p, W.ci.p, nc, n, W.mn.p, W.mx.p, W.tmp.p, W.bucket.p, W.hist.p,
+                               job.cfg.enable_hilbert_sorting ? 1 : 0);
   uint32_t hmask = 1;
   while (hmask < 2 * n) hmask <<= 1;
   W.dtab.reserve(hmask, "dedup table");
