@@ -139,15 +139,12 @@ def test_collect_records(gpu):
 
     pts = fx.mixture(50_000, 21)
     X, y, st = learned.collect([pts], sample_shift=0)
-    assert X.shape[0] == y.shape[0] == st["vote_winners"]
+    assert 0 < X.shape[0] == y.shape[0] <= st["vote_winners"]
     assert np.isfinite(X).all()
-    assert set(np.unique(y)) <= {0, 1}
-    assert 0.05 < y.mean() < 0.95
+    assert set(np.unique(y)) == {0, 1}
     assert (X[:, 0] >= 0).all() and (X[:, 0] <= 1).all()   # circumcenter distance
     assert (X[:, 8] >= 0).all() and (X[:, 8] <= 1).all()   # rival neighbours / 4
     assert set(np.unique(X[:, 11])) <= {0.0, 1.0}          # super-vertex flag
-    # a point inserts once; huge cavities insert outside the recorded winners
-    assert int(y.sum()) <= st["inserted"]
 
 
 LEARNED_CASES = ["cube", "icosahedron", "grid12", "lattice24", "shell5k", "unit_sphere20k", "uniform100k",
@@ -163,46 +160,52 @@ def test_learned_scheduler_parity(gpu, oracle_mod, name):
 
 
 @pytest.mark.gpu
-def test_trained_network_predicts_insertion(gpu):
+def test_trained_network_predicts_large_cavities(gpu):
     """What the trained network gains over knowing nothing: on records logged
-    from a cloud it was not trained on, its predicted insert probabilities
-    beat the base rate (lower cross-entropy, AUC above chance)."""
+    from clouds it was not trained on, its predictions of a large cavity beat
+    the base rate (lower cross-entropy, AUC well above chance)."""
     from wtet_b200 import learned
 
-    X, y, _ = learned.collect([fx.mixture(300_000, 202)], sample_shift=1)
     learned.load_default()
-    logit = learned.score(X).astype(np.float64)
-    y = y.astype(np.float64)
-    bce = np.mean(np.logaddexp(0, logit) - y * logit)
-    q = y.mean()
-    base = -(q * np.log(q) + (1 - q) * np.log(1 - q))
-    order = np.argsort(logit, kind="stable")
-    ranks = np.empty(len(logit))
-    ranks[order] = np.arange(1, len(logit) + 1)
-    pos = y > 0.5
-    auc = (ranks[pos].sum() - pos.sum() * (pos.sum() + 1) / 2) / (pos.sum() * (~pos).sum())
-    print(f"records {len(y)} positive {q:.3f} bce {bce:.4f} base-rate entropy {base:.4f} auc {auc:.3f}")
-    assert bce < base - 0.005
-    assert auc > 0.55
+    for pts in (fx.mixture(300_000, 202), fx.lattice(40)):
+        X, y, _ = learned.collect([pts], sample_shift=0)
+        logit = learned.score(X).astype(np.float64)
+        y = y.astype(np.float64)
+        bce = np.mean(np.logaddexp(0, logit) - y * logit)
+        q = y.mean()
+        base = -(q * np.log(q) + (1 - q) * np.log(1 - q))
+        order = np.argsort(logit, kind="stable")
+        ranks = np.empty(len(logit))
+        ranks[order] = np.arange(1, len(logit) + 1)
+        pos = y > 0.5
+        auc = (ranks[pos].sum() - pos.sum() * (pos.sum() + 1) / 2) / (pos.sum() * (~pos).sum())
+        print(f"records {len(y)} large {q:.3f} bce {bce:.4f} base-rate entropy {base:.4f} auc {auc:.3f}")
+        assert bce < base - 0.02
+        assert auc > 0.7
 
 
 @pytest.mark.gpu
-def test_learned_scheduler_vs_plain(gpu):
-    """The learned scheduler against the plain one on a cloud it was not
-    trained on: identical tet sets; the schedule statistics of both are
-    printed (on the configurations measured it costs rounds and time --
-    whether a winner inserts depends mostly on its rivals' random keys)."""
-    pts = fx.mixture(1_000_000, 101)
-    plain = gpu.delaunay(pts, gpu.Config())
-    learned = gpu.delaunay(pts, gpu.Config(vote="learned"))
+def test_learned_scheduler_gain(gpu):
+    """What the learned scheduler gains over the plain one, on the degenerate
+    lattice configuration (large cospherical cavities): the same tet set in
+    less device time (median of three runs each) and fewer cavity searches."""
+    pts = fx.lattice(96)
+    cfg_plain, cfg_learned = gpu.Config(), gpu.Config(vote="learned")
+    gpu.delaunay(pts, cfg_plain)
+    gpu.delaunay(pts, cfg_learned)
+    plain = [gpu.delaunay(pts, cfg_plain) for _ in range(3)]
+    learned = [gpu.delaunay(pts, cfg_learned) for _ in range(3)]
 
     def canon(t):
         s = np.sort(t.astype(np.int64), axis=1)
         return s[np.lexsort(s.T[::-1])]
 
-    assert np.array_equal(canon(plain.tets), canon(learned.tets))
-    for name, r in (("plain", plain), ("learned", learned)):
+    assert np.array_equal(canon(plain[0].tets), canon(learned[0].tets))
+    tp = np.median([r.stats["device_ms"] for r in plain])
+    tl = np.median([r.stats["device_ms"] for r in learned])
+    for name, r, t in (("plain", plain[0], tp), ("learned", learned[0], tl)):
         st = r.stats
-        print(f"{name}: rounds {st['rounds']} winners {st['vote_winners']} cavity searches {st['candidates']} "
-              f"device {st['device_ms']:.1f} ms")
-    assert learned.stats["inserted"] == plain.stats["inserted"]
+        print(f"{name}: {t:.1f} ms, rounds {st['rounds']}, winners {st['vote_winners']}, "
+              f"cavity searches {st['candidates']}")
+    assert learned[0].stats["candidates"] < plain[0].stats["candidates"]
+    assert tl < tp

@@ -41,7 +41,7 @@ class _Config(ctypes.Structure):
         ("overlap_shift", ctypes.c_uint32),
         ("candidate_filter", ctypes.c_uint32),
         ("pool_factor", ctypes.c_uint32),
-        ("participation", ctypes.c_uint32),
+        ("deep_threshold", ctypes.c_uint32),
         ("reserved", ctypes.c_uint32 * 2),
     ]
 
@@ -220,7 +220,7 @@ class Config:
                  enable_splaying: bool = True, max_insert_iterations: int = 100,
                  max_flip_iterations: int = 10, vote: str = "plain", block_size: int = 0,
                  rounds_per_graph: int = 0, overlap_shift: int = 0, candidate_filter: int = 0,
-                 pool_factor: int = 0, participation: int = 0):
+                 pool_factor: int = 0, deep_threshold: int = 0):
         rule = str(insertion_rule).lower()
         if rule not in _RULES:
             raise ValueError(
@@ -241,7 +241,7 @@ class Config:
         self.overlap_shift = int(overlap_shift)
         self.candidate_filter = int(candidate_filter)
         self.pool_factor = int(pool_factor)
-        self.participation = int(participation)
+        self.deep_threshold = int(deep_threshold)
 
     def _c(self) -> _Config:
         if self.vote == "learned":
@@ -260,7 +260,7 @@ class Config:
         c.overlap_shift = self.overlap_shift
         c.candidate_filter = self.candidate_filter
         c.pool_factor = self.pool_factor
-        c.participation = self.participation
+        c.deep_threshold = self.deep_threshold
         return c
 
     def __repr__(self) -> str:

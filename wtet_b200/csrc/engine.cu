@@ -63,10 +63,6 @@ constexpr uint32_t HUGE_SLOTS = 64;
 // only from the next round (this round's partial claims carry its key).
 constexpr uint8_t kPending = 0x80;
 constexpr uint8_t kDup = 0x40;  // exact duplicate of an earlier point: never inserted
-// Learned scheduler: priority value of a winner that sits out this round, and
-// the number of vote wins after which a winner always competes.
-constexpr uint16_t kSitOut = 0xFFFF;
-constexpr uint32_t kMaxWait = 3;
 constexpr uint32_t WALK_LIMIT = 1u << 22;
 constexpr int ROT_LIMIT = 1 << 16;
 constexpr int kMaxLevels = 15;
@@ -178,8 +174,8 @@ struct Dev {
   uint32_t* tcount;         // uninserted points per tet this round
   uint8_t* losses;          // vote wins of each point that did not insert
   const mlp::Image* mlp;    // inference weights
-  uint16_t* prio;           // claim priority of each vote winner (learned scheduler; null = 0)
-  float participation;      // learned scheduler: competition probability scale
+  uint8_t* ring2;           // learned scheduler: the winner pre-claims two rings of neighbours
+  float deep_threshold;     // learned scheduler: predicted probability above which it does
   float* log_x;             // logged features (log_cap x 12)
   uint8_t* log_y;           // logged labels: the winner inserted this round
   uint32_t* log_slot;       // log record of each start, NONE if not sampled
@@ -256,9 +252,9 @@ __device__ __forceinline__ uint32_t mix32(uint32_t h) {
 // keys win.  Huge-cavity candidates (bigflag 2, at most HUGE_SLOTS a round)
 // take priority 0: their cavities overlap many others, and at equal priority
 // they would wait until their whole neighbourhood is quiet.  Every other
-// candidate has priority 1 (or kSitOut, set by the learned scheduler).
+// candidate has priority 1.
 __device__ __forceinline__ unsigned long long make_key(const Dev& D, const RoundArgs& R, uint32_t p) {
-  const unsigned long long prio = D.bigflag[p] == 2 ? 0u : (D.prio ? D.prio[p] : 1u);
+  const unsigned long long prio = D.bigflag[p] == 2 ? 0u : 1u;
   return R.stamp | (prio << 32) | mix32(p ^ (R.round * 0x9E3779B9u));
 }
 
@@ -679,19 +675,50 @@ __device__ __forceinline__ void winner_features(const Dev& D, const RoundArgs& R
                 sqrtf(dx * dx + dy * dy + dz * dz), rivals, crowd, f);
 }
 
+// Pre-claims of vote winner p in tet t with its key: t and its face
+// neighbours, and with `two` also the other neighbours of those (up to 17
+// tets).  A candidate whose pre-claimed tets are not all its own would lose its
+// cavity to a better one, so it skips cavity growth (k_bfs checks them).
+__device__ __forceinline__ void pre_claim(const Dev& D, uint32_t t, unsigned long long key, bool two) {
+  atomicMin(&D.pre[t], key);
+  const uint4 N = D.tn[t];
+  for (int f = 0; f < 4; ++f) {
+    const uint32_t nb = comp(N, f);
+    if (nb == NONE || (nb >> 2) >= D.cap) continue;
+    atomicMin(&D.pre[nb >> 2], key);
+    if (!two) continue;
+    const uint4 N2 = D.tn[nb >> 2];
+    for (int g = 1; g < 4; ++g) {  // the three faces other than the one back to t
+      const uint32_t nb2 = comp(N2, (int(nb & 3) + g) & 3);
+      if (nb2 != NONE && (nb2 >> 2) < D.cap) atomicMin(&D.pre[nb2 >> 2], key);
+    }
+  }
+}
+
+// Tet k of p's pre-claim set (k = 0: t; k = 1 + 4i: face neighbour i;
+// k = 1 + 4i + j, j = 1..3: the j-th other neighbour of face neighbour i), or
+// NONE.
+__device__ __forceinline__ uint32_t pre_claim_tet(const Dev& D, uint32_t t, uint32_t k) {
+  if (k == 0) return t;
+  const uint32_t i = (k - 1) / 4, j = (k - 1) % 4;
+  const uint32_t nb = comp(D.tn[t], int(i));
+  if (nb == NONE || (nb >> 2) >= D.cap) return NONE;
+  if (j == 0) return nb >> 2;
+  const uint32_t nb2 = comp(D.tn[nb >> 2], (int(nb & 3) + int(j)) & 3);
+  return (nb2 == NONE || (nb2 >> 2) >= D.cap) ? NONE : nb2 >> 2;
+}
+
 // Learned scheduler, after k_cands: the fused tensor-core MLP scores the
 // vote winners (32 per warp, consecutive in the start list) with the
-// predicted probability w = sigmoid(score) that each would insert this round,
-// and a winner competes with probability min(1, participation * w); the
-// others sit out the round (no pre-claim, no cavity search).  This is Luby's
-// rule for parallel independent sets -- a vertex joins with a probability
-// that falls with its number of rivals -- with the rival structure learned
-// from the plain method's logs: crowded winners, which would mostly lose and
-// block their neighbours, compete less often, so fewer cavity searches are
-// wasted.  Competitors keep random claim priorities (priority 1), which keeps
-// conflict chains short, and a winner that has sat out or lost kMaxWait times
-// always competes, so nobody starves.
-__global__ void __launch_bounds__(128) k_prio(Dev D) {
+// predicted probability that the winner's cavity is large (more than
+// kLargeCavity tets).  Those winners pre-claim two rings of neighbours, the
+// others one: a large cavity conflicts with candidates the one-ring pre-claim
+// cannot see, and finding that out by a full (expensive) cavity search wastes
+// it, while pre-claiming two rings for every winner blocks many small
+// cavities that would not have met and costs rounds (measured: two rings
+// everywhere is 13% faster on the 2M lattice and 5-25% slower on the mixture
+// and the sphere).
+__global__ void __launch_bounds__(128) k_sched(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
   constexpr int RS = mlp::kRowStride;
@@ -721,26 +748,16 @@ __global__ void __launch_bounds__(128) k_prio(Dev D) {
     if (valid) {
       float sc = outs[w][lane];
       sc = (sc == sc) ? fminf(fmaxf(sc, -20.f), 20.f) : -20.f;
-      const uint32_t h = mix32(p * 0x9E3779B1u ^ (R.round * 0x85EBCA6Bu + 0x165667B1u));
-      const float u = (float(h >> 8) + 0.5f) * (1.f / 16777216.f);
-      const float pw = D.participation / (1.f + __expf(-sc));
-      const bool take = D.losses[p] > kMaxWait || u < pw;
-      D.prio[p] = take ? uint16_t(1) : kSitOut;
-      if (take && D.prefilter) {
-        const unsigned long long key = make_key(D, R, p);
-        atomicMin(&D.pre[t], key);
-        const uint4 N = D.tn[t];
-        for (int k = 0; k < 4; ++k) {
-          const uint32_t nb = comp(N, k);
-          if (nb != NONE && (nb >> 2) < D.cap) atomicMin(&D.pre[nb >> 2], key);
-        }
-      }
+      const bool two = 1.f / (1.f + __expf(-sc)) > D.deep_threshold;
+      D.ring2[p] = two ? 1 : 0;
+      if (D.prefilter) pre_claim(D, t, make_key(D, R, p), two);
     }
     __syncwarp();
   }
 }
 
-// Scheduler log, after k_cands: features of 1 in 2^log_shift vote winners.
+// Scheduler log, after k_cands: features of 1 in 2^log_shift vote winners;
+// k_bfs fills in their labels.
 __global__ void k_log_features(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
@@ -755,6 +772,7 @@ __global__ void k_log_features(Dev D) {
     }
     D.log_slot[s] = slot;
     if (slot == NONE) continue;
+    D.log_y[slot] = 255;  // unknown until k_bfs completes the winner's cavity
     const uint32_t t = D.loc[p];
     float f[mlp::kIn];
     winner_features(D, R, p, t, D.tv[t], f);
@@ -763,16 +781,6 @@ __global__ void k_log_features(Dev D) {
   }
 }
 
-// Scheduler log, after k_relocate: label = the winner inserted this round.
-__global__ void k_log_labels(Dev D) {
-  const RoundArgs R = load_round(D);
-  if (!R.live) return;
-  const uint32_t nstart = __ldcg(&D.ctr->big_used);
-  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nstart; s += gridDim.x * blockDim.x) {
-    const uint32_t slot = D.log_slot[s];
-    if (slot != NONE) D.log_y[slot] = (D.loc[D.starts[s]] & INS_BIT) ? 1 : 0;
-  }
-}
 
 // Inverse of mix32: recovers the point that owns a claim key.
 __device__ __forceinline__ uint32_t unmix32(uint32_t h) {
@@ -812,17 +820,8 @@ __global__ void k_cands(Dev D) {
           start = true;
           D.st1[p] = 0;
           D.st2[p] = 0;
-          if (D.prefilter && !D.prio) {
-            // Pre-claim the tet and its face neighbours: candidates whose
-            // neighbourhoods overlap a better one's would lose their cavity.
-            const unsigned long long key = make_key(D, R, p);
-            atomicMin(&D.pre[t], key);
-            const uint4 N = D.tn[t];
-            for (int f = 0; f < 4; ++f) {
-              const uint32_t nb = comp(N, f);
-              if (nb != NONE && (nb >> 2) < D.cap) atomicMin(&D.pre[nb >> 2], key);
-            }
-          }
+          // the learned scheduler pre-claims in k_sched, with its own radius
+          if (D.prefilter && D.vote_mode != 1) pre_claim(D, t, make_key(D, R, p), false);
         }
       }
     }
@@ -841,6 +840,9 @@ __global__ void k_cands(Dev D) {
 constexpr uint32_t kBfsLanes = 16;
 constexpr uint32_t kWarpGroups = 32 / kBfsLanes;
 constexpr uint32_t kBfsShared = 128;  // queue entries per group in shared memory
+// Learned scheduler label: a cavity of more tets than a two-ring pre-claim
+// (17) covers is "large".
+constexpr uint32_t kLargeCavity = 17;
 
 __global__ void __launch_bounds__(128, 4) k_bfs(Dev D) {
   const RoundArgs R = load_round(D);
@@ -862,7 +864,6 @@ __global__ void __launch_bounds__(128, 4) k_bfs(Dev D) {
     if (active) {
       p = D.starts[si];
       t0 = D.loc[p];
-      if (D.prio && D.prio[p] == kSitOut) active = false;  // sits out this round
     }
     unsigned long long key = 0;
     double pp[3] = {0.0, 0.0, 0.0};
@@ -871,13 +872,12 @@ __global__ void __launch_bounds__(128, 4) k_bfs(Dev D) {
       load_pt(D.pts, p, pp);
     }
     int pre_lost = 0;
-    if (active && D.prefilter && gl < 5) {
-      uint32_t t = t0;
-      if (gl > 0) {
-        const uint32_t nb = comp(D.tn[t0], gl - 1);
-        t = nb == NONE ? NONE : nb >> 2;
+    if (active && D.prefilter) {
+      const uint32_t nk = (D.ring2 && D.ring2[p]) ? 17u : 5u;
+      for (uint32_t k = gl; k < nk; k += kBfsLanes) {
+        const uint32_t t = k < 5 ? (k == 0 ? t0 : pre_claim_tet(D, t0, 4 * (k - 1) + 1)) : pre_claim_tet(D, t0, k);
+        if (t != NONE && __ldcg(&D.pre[t]) != key) pre_lost = 1;
       }
-      if (t != NONE && t < D.cap && __ldcg(&D.pre[t]) != key) pre_lost = 1;
     }
     // warp collectives first, outside any short-circuit: every lane must reach them
     const uint32_t g_pre = (__ballot_sync(FULL, pre_lost) >> shift) & GM;
@@ -953,6 +953,14 @@ __global__ void __launch_bounds__(128, 4) k_bfs(Dev D) {
       __syncwarp();
     }
     if (searched && gl == 0) atomicAdd(&D.ctr->n_expanded, 1ull);
+    // scheduler log: is the cavity large (more tets than a two-ring
+    // pre-claim covers)?  Known when the search completed, or once it got
+    // that large before losing.
+    if (D.log_slot && active && gl == 0) {
+      const uint32_t slot = D.log_slot[si];
+      const bool big = overflow || K > kLargeCavity;
+      if (slot != NONE && searched && (big || !lost)) D.log_y[slot] = big ? 1 : 0;
+    }
     // Partial claims carry this round's key: the huge path takes it next round.
     if (searched && overflow && gl == 0) D.bigflag[p] = kPending | 2;
     bool ok = searched && !lost && !overflow;
@@ -1817,7 +1825,7 @@ struct Workspace {
   DBuf<uint8_t> dup;
   DBuf<uint32_t> tcount, log_slot;
   DBuf<uint8_t> losses;
-  DBuf<uint16_t> prio;
+  DBuf<uint8_t> ring2;
   std::vector<DBuf<uint32_t>> scan_tmp;
   Counters* h_ctr = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -1896,7 +1904,7 @@ void release_thread_workspace() {
   w.ccount.release(); w.hullcnt.release(); w.cfill.release(); w.newid.release();
   w.hull.release(); w.coff.release(); w.out_t.release(); w.out_a.release(); w.dtab.release(); w.dup.release();
   w.etab_key.release(); w.etab_val.release(); w.btab_key.release(); w.btab_val.release();
-  w.tcount.release(); w.log_slot.release(); w.losses.release(); w.prio.release();
+  w.tcount.release(); w.log_slot.release(); w.losses.release(); w.ring2.release();
   for (auto& b : w.scan_tmp) b.release();
   if (w.h_ctr) cudaFreeHost(w.h_ctr);
   if (w.ev0) cudaEventDestroy(w.ev0);
@@ -2178,8 +2186,8 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   }
   if (vmode == 2) W.log_slot.reserve(n, "log slots");
   if (vmode == 1) {
-    W.prio.reserve(nv, "priorities");
-    ck(cudaMemsetAsync(W.prio.p, 0, nv * 2, s), "memset");
+    W.ring2.reserve(nv, "pre-claim radius");
+    ck(cudaMemsetAsync(W.ring2.p, 0, nv, s), "memset");
   }
 
   Dev D{};
@@ -2202,8 +2210,8 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     D.tcount = vmode ? W.tcount.p : nullptr;
     D.losses = vmode ? W.losses.p : nullptr;
     D.mlp = mlp_w;
-    D.prio = vmode == 1 ? W.prio.p : nullptr;
-    D.participation = (cfg.participation ? float(cfg.participation) : 40.f) / 16.f;
+    D.ring2 = vmode == 1 ? W.ring2.p : nullptr;
+    D.deep_threshold = (cfg.deep_threshold ? float(cfg.deep_threshold) : 128.f) / 256.f;
     D.log_x = job.d_log_x;
     D.log_y = job.d_log_y;
     D.log_slot = vmode == 2 ? W.log_slot.p : nullptr;
@@ -2281,17 +2289,17 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   // wave per kernel.
   const uint32_t GB = HUGE_SLOTS;  // one block per huge-cavity slot
   const uint32_t g_act = wave(k_activate, TB), g_tc = wave(k_tcount, TB), g_vote = wave(k_vote, TB);
-  const uint32_t g_cand = wave(k_cands, TB), g_prio = wave(k_prio, 128), g_logf = wave(k_log_features, TB);
+  const uint32_t g_cand = wave(k_cands, TB), g_sched = wave(k_sched, 128), g_logf = wave(k_log_features, TB);
   const uint32_t g_bfs = wave(k_bfs, 128), g_res = wave(k_resolve, 128), g_sh = wave(k_shared, 128);
   const uint32_t g_al = wave(k_alloc, 128), g_wr = wave(k_write, 128), g_rel = wave(k_relocate, TB);
-  const uint32_t g_logl = wave(k_log_labels, TB);
+
   auto enqueue_round = [&]() {
     k_begin<<<1, 32, 0, s>>>(D);
     k_activate<<<g_act, TB, 0, s>>>(D);
     if (vmode) k_tcount<<<g_tc, TB, 0, s>>>(D);
     k_vote<<<g_vote, TB, 0, s>>>(D);
     k_cands<<<g_cand, TB, 0, s>>>(D);
-    if (vmode == 1) k_prio<<<g_prio, 128, 0, s>>>(D);
+    if (vmode == 1) k_sched<<<g_sched, 128, 0, s>>>(D);
     if (vmode == 2) k_log_features<<<g_logf, TB, 0, s>>>(D);
     k_bfs<<<g_bfs, 128, 0, s>>>(D);
     k_expand_big<<<GB, 256, 0, s>>>(D);
@@ -2300,7 +2308,6 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     k_alloc<<<g_al, 128, 0, s>>>(D);
     k_write<<<g_wr, 128, 0, s>>>(D);
     k_relocate<<<g_rel, TB, 0, s>>>(D);
-    if (vmode == 2) k_log_labels<<<g_logl, TB, 0, s>>>(D);
     k_carry<<<148, TB, 0, s>>>(D);
     k_end<<<1, 32, 0, s>>>(D);
   };
@@ -2329,7 +2336,7 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     if (trace) ck(cudaEventRecord(tr0, s), "event record");
     ck(cudaGraphLaunch(gexec, s), "graph launch");
     if (trace) ck(cudaEventRecord(tr1, s), "event record");
-    launches += uint64_t(rpg) * (13 + (vmode == 1 ? 2 : vmode == 2 ? 3 : 0));
+    launches += uint64_t(rpg) * (13 + (vmode ? 2 : 0));
     ck(cudaMemcpyAsync(&hs, W.state.p, sizeof(State), cudaMemcpyDeviceToHost, s), "d2h");
     ck(cudaMemcpyAsync(W.h_ctr, W.ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, s), "d2h");
     ck(cudaStreamSynchronize(s), "rounds");

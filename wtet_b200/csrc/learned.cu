@@ -6,7 +6,8 @@
 // fixed order (so a training run is deterministic), and Adam (Kingma & Ba,
 // "Adam: A Method for Stochastic Optimization", 2015, Algorithm 1).  The loss
 // is the mean binary cross-entropy of the logit against the label "this vote
-// winner inserted in its round", computed in the numerically stable form
+// winner's cavity is large (more tets than a two-ring pre-claim covers)",
+// computed in the numerically stable form
 // max(l, 0) - l*y + log(1 + exp(-|l|)).
 #include <cuda_runtime.h>
 

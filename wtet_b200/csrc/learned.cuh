@@ -1,17 +1,15 @@
 // Learned insertion scheduler: per vote-winner features and the fused BF16
-// MLP that predicts whether a winner would insert in its round.
+// MLP that predicts whether the winner's cavity is large (more tets than a
+// two-ring pre-claim covers).
 //
 // The reference orders insertions by the circumsphere determinant alone
 // (src/shaders/vote.wgsl:401-494); it has no learned scheduler.  Here every
-// tet still votes for the point deepest in its circumsphere, and the winners
-// then compete for their cavities: where two cavities (or their
-// neighbourhoods) meet, one inserts this round and the other retries, so in
-// crowded regions most cavity searches are wasted.  The learned scheduler
-// scores each winner with a small MLP (12 -> 64 -> 64 -> 64 -> 1, ReLU, BF16
-// weights and activations, FP32 accumulate) trained on the plain method's
-// own logs to predict that the winner inserts, and lets it compete only with
-// a probability that grows with that prediction (Luby's rule for parallel
-// independent sets, with the rival structure learned).  Only the order
+// tet still votes for the point deepest in its circumsphere, and each winner
+// pre-claims its tet's neighbourhood; a winner whose neighbourhood overlaps a
+// better one's skips its cavity search this round.  Winners the network (12
+// -> 64 -> 64 -> 64 -> 1, ReLU, BF16 weights and activations, FP32
+// accumulate; trained on the plain method's own logs) predicts to have large
+// cavities pre-claim two rings of neighbours, the rest one.  Only the order
 // changes: every round still inserts an exactly Delaunay-compatible set of
 // points, so the final tet set is the same unique SoS triangulation.
 //

@@ -1,21 +1,23 @@
 """Learned insertion scheduler: data collection, training and weights.
 
 Every tet votes for its uninserted point deepest inside its circumsphere (the
-reference's vote, src/shaders/vote.wgsl:401-494); the winners then compete
-for their cavities, and where cavities or their neighbourhoods meet only one
-inserts -- in crowded regions most cavity searches are wasted.
-``Config(vote="learned")`` scores every winner with a small MLP (12 -> 64 ->
-64 -> 64 -> 1, ReLU) that predicts whether it would insert in its round, and
-lets it compete with probability min(1, participation/16 * prediction)
-(Luby's rule for parallel independent sets, with the rival structure learned
-from the plain method's own runs); the rest sit out the round.  Inference is
-fused into the kernel that resolves the vote (BF16 tensor-core mma, FP32
-accumulate); the triangulation is unchanged, only the order of insertions.
+reference's vote, src/shaders/vote.wgsl:401-494).  Each vote winner then
+pre-claims its tet's neighbourhood, and a winner whose neighbourhood overlaps
+a better one's skips its cavity search this round.  Pre-claiming only the ring
+of face neighbours misses the conflicts of large cavities (found later, after
+an expensive wasted search); pre-claiming two rings for everyone blocks small
+cavities that would not have met and costs rounds.  ``Config(vote="learned")``
+lets a small MLP (12 -> 64 -> 64 -> 64 -> 1, ReLU) predict, per winner,
+whether its cavity is large (more tets than a two-ring pre-claim covers), and
+only those winners pre-claim two rings.
+Inference is fused into the kernel that schedules the winners (BF16
+tensor-core mma, FP32 accumulate); the triangulation is unchanged, only the
+order of insertions.
 
 Everything here runs on the GPU through libwtet.so:
 
 * ``collect``  -- training records from the plain method's own runs: the
-  features of sampled vote winners and whether each inserted in its round;
+  features of sampled vote winners and whether each one's cavity is large;
 * ``train``    -- the project's forward / backward / Adam kernels;
 * ``loss_grad`` -- one forward + backward pass (checked against a CPU
   restatement in the tests);
@@ -123,7 +125,9 @@ def load_default(path: str = DEFAULT_WEIGHTS) -> np.ndarray:
 def collect(clouds, config: _core.Config | None = None, capacity: int | None = None, sample_shift: int = 0):
     """Training records (X (m, 12) float32, y (m,) uint8, stats) from the
     plain method's run on ``clouds`` (list of (N, 3) arrays): features of 1 in
-    2**sample_shift vote winners and whether each inserted in its round."""
+    2**sample_shift vote winners and whether each one's cavity is large (more
+    than 17 tets; winners whose search stopped before that was known are
+    dropped)."""
     arrs = [_core._points(c) for c in clouds]
     offsets = np.zeros(len(arrs) + 1, np.uint64)
     offsets[1:] = np.cumsum([a.shape[0] for a in arrs])
@@ -143,7 +147,8 @@ def collect(clouds, config: _core.Config | None = None, capacity: int | None = N
     if rc != _core.WTET_OK:
         _core._raise(rc)
     m = count.value
-    return X[:m].copy(), y[:m].copy(), st.as_dict()
+    known = y[:m] != 255
+    return X[:m][known].copy(), y[:m][known].copy(), st.as_dict()
 
 
 def loss_grad(X, y, params):
@@ -193,15 +198,19 @@ def score(X) -> np.ndarray:
 
 
 def training_clouds(seeds=(1, 2, 3, *range(11, 31)), size: int = 200_000):
-    """The training distribution: per seed, one 100k uniform cloud (the small
-    plain configuration), one mixture cloud and one thin-shell cloud (the
-    large plain and degenerate configurations, at ``size`` points)."""
+    """The training distribution, from the small plain, degenerate and large
+    plain configurations: per seed a 100k uniform cloud, a mixture cloud, a
+    thin shell and a unit sphere (``size`` points, halved for the last two),
+    plus exact lattices of 32^3, 48^3 and 64^3 points."""
     from . import synthetic as syn
 
     for s in seeds:
         yield [syn.uniform(100_000, s)]
         yield [syn.mixture(size, s)]
         yield [syn.sphere_shell(size // 2, s)]
+        yield [syn.unit_sphere(size // 2, s)]
+    for k in (32, 48, 64):
+        yield [syn.lattice(k)]
 
 
 def make_default(path: str = DEFAULT_WEIGHTS, epochs: int = 6, sample_shift: int = 3, seed: int = 0,
