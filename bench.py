@@ -406,6 +406,23 @@ def variants(wt, args):
             ("vote_winners", int(res[v][0].stats["vote_winners"])),
             ("cavity_searches", int(res[v][0].stats["candidates"])))},
     }
+    # the degenerate configuration, where large cavities make searches expensive
+    lat = make_workload("lattice2M")[0]
+    resl = {}
+    for vote in ("plain", "learned"):
+        cfg = wt.Config(vote=vote)
+        wt.delaunay(lat, cfg)
+        runs = [wt.delaunay(lat, cfg) for _ in range(2)]
+        resl[vote] = (runs[-1], float(np.median([r.stats["device_ms"] for r in runs])))
+    out["learned_lattice"] = {
+        "workload": "lattice2M",
+        "same_tet_set": _canon_digest(resl["plain"][0].tets) == _canon_digest(resl["learned"][0].tets),
+        **{f"{v}_{k}": val for v in ("plain", "learned") for k, val in (
+            ("mpts", round(len(lat) / (resl[v][1] * 1e3), 3)),
+            ("device_ms", round(resl[v][1], 1)),
+            ("rounds", int(resl[v][0].stats["rounds"])),
+            ("cavity_searches", int(resl[v][0].stats["candidates"])))},
+    }
     clouds = make_workload("batched")
     n = sum(len(c) for c in clouds)
     wt.delaunay_batched(clouds)

@@ -73,7 +73,7 @@ typedef struct wtet_config {
   uint32_t pool_factor;            /* cavity-pool entries per point (default 24, 4..64) */
   uint32_t deep_threshold;         /* learned scheduler: a vote winner whose predicted probability
                                       of a large cavity exceeds deep_threshold/256 pre-claims two
-                                      rings of neighbours; 0 = default (128) */
+                                      rings of neighbours; 0 = default (64, i.e. 1/4) */
   uint32_t reserved[2];
 } wtet_config;
 

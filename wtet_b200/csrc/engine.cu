@@ -2211,7 +2211,7 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     D.losses = vmode ? W.losses.p : nullptr;
     D.mlp = mlp_w;
     D.ring2 = vmode == 1 ? W.ring2.p : nullptr;
-    D.deep_threshold = (cfg.deep_threshold ? float(cfg.deep_threshold) : 128.f) / 256.f;
+    D.deep_threshold = (cfg.deep_threshold ? float(cfg.deep_threshold) : 64.f) / 256.f;
     D.log_x = job.d_log_x;
     D.log_y = job.d_log_y;
     D.log_slot = vmode == 2 ? W.log_slot.p : nullptr;
