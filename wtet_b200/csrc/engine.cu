@@ -539,7 +539,7 @@ __global__ void k_init_clouds(const CloudInfo* ci, uint32_t nc, Dev D) {
 // stride earlier on the Morton curve (a point of an earlier stratum: its tet
 // once inserted, else the tet that still contains it).  The located points are
 // appended to the uninserted list at position `base`.
-__global__ void __launch_bounds__(256, 3) k_activate(Dev D) {
+__global__ void __launch_bounds__(256, 4) k_activate(Dev D) {
   RoundArgs R = load_round(D);
   if (!R.live) return;
   volatile State* S = D.st;
@@ -844,7 +844,7 @@ constexpr uint32_t kBfsShared = 128;  // queue entries per group in shared memor
 // (17) covers is "large".
 constexpr uint32_t kLargeCavity = 17;
 
-__global__ void __launch_bounds__(128, 6) k_bfs(Dev D) {
+__global__ void __launch_bounds__(128, 8) k_bfs(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
   constexpr uint32_t FULL = 0xFFFFFFFFu, GM = (kBfsLanes == 32) ? 0xFFFFFFFFu : ((1u << kBfsLanes) - 1u);
@@ -1103,7 +1103,7 @@ __global__ void k_resolve(Dev D) {
 // Delaunay: the better winner q must lie outside the circumsphere of the
 // worse winner p's new tet on f (then either insertion order gives the same
 // tets).  The worse one of a violating pair steps back.
-__global__ void __launch_bounds__(128, 6) k_shared(Dev D) {
+__global__ void __launch_bounds__(128, 8) k_shared(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
   const uint32_t lane = threadIdx.x & 31;
@@ -1244,7 +1244,7 @@ __device__ __forceinline__ uint32_t edge_hash(uint32_t a, uint32_t b, uint32_t m
   return mix32(a * 0x9E3779B9u ^ b) & mask;
 }
 
-__global__ void __launch_bounds__(128, 6) k_write(Dev D) {
+__global__ void __launch_bounds__(128, 8) k_write(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
   __shared__ unsigned long long ekey[4][kEdgeSlots];
@@ -1428,7 +1428,7 @@ __global__ void __launch_bounds__(128, 6) k_write(Dev D) {
 
 // Clears the votes, relocates points whose tet was retired, and compacts the
 // uninserted list.
-__global__ void __launch_bounds__(256, 3) k_relocate(Dev D) {
+__global__ void __launch_bounds__(256, 4) k_relocate(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
   uint32_t steps = 0;
