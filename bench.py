@@ -353,7 +353,7 @@ def run_gpu(args):
 # dram__bytes_write.sum over all launches, --cache-control none), scaled by the
 # point count for the larger clouds of the same distribution
 # (profiles/launch_list_mixture1M.md).
-_TRAFFIC_1M_MIXTURE = 37.434e9
+_TRAFFIC_1M_MIXTURE = 49.934e9
 TRAFFIC: dict = {
     "mixture1M": _TRAFFIC_1M_MIXTURE,
     "mixture8M": 8 * _TRAFFIC_1M_MIXTURE,

@@ -539,7 +539,7 @@ __global__ void k_init_clouds(const CloudInfo* ci, uint32_t nc, Dev D) {
 // stride earlier on the Morton curve (a point of an earlier stratum: its tet
 // once inserted, else the tet that still contains it).  The located points are
 // appended to the uninserted list at position `base`.
-__global__ void __launch_bounds__(256, 4) k_activate(Dev D) {
+__global__ void __launch_bounds__(512, 2) k_activate(Dev D) {
   RoundArgs R = load_round(D);
   if (!R.live) return;
   volatile State* S = D.st;
@@ -1428,7 +1428,7 @@ __global__ void __launch_bounds__(128, 8) k_write(Dev D) {
 
 // Clears the votes, relocates points whose tet was retired, and compacts the
 // uninserted list.
-__global__ void __launch_bounds__(256, 4) k_relocate(Dev D) {
+__global__ void __launch_bounds__(512, 2) k_relocate(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
   uint32_t steps = 0;
