@@ -12,12 +12,22 @@
 // equivalent to some sequential order.  The result is therefore the unique
 // SoS Delaunay triangulation, with no flip failures and nothing left to repair.
 //
-// Round structure (one insertion round over all clouds of a job):
+// Round structure (one insertion round over all clouds of a job; 13 kernels
+// replayed from a CUDA graph, 15 with the learned scheduler):
+//   k_begin       start the next stratum when the current one has thinned
+//   k_activate    locate the new stratum's points (walk from the curve
+//                 predecessor's tet)
 //   k_vote        each uninserted point votes for its tet (64-bit atomicMax of
 //                 score | ~point, src/shaders/vote.wgsl semantics)
-//   k_cands/k_bfs each vote winner grows its cavity by warp-cooperative BFS
-//                 with exact insphere, claiming cavity tets by 64-bit atomicMin
-//                 of a round-stamped priority key
+//   k_cands       the winner of each tet becomes a candidate and pre-claims
+//                 its tet's neighbourhood with its claim key
+//   (k_tcount, k_sched: the learned scheduler sets each winner's pre-claim
+//                 radius from the fused BF16 MLP instead)
+//   k_bfs         candidates whose pre-claims all hold grow their cavities by
+//                 breadth-first search with exact insphere (16 lanes per
+//                 candidate), claiming cavity tets by 64-bit atomicMin of a
+//                 round-stamped key; k_expand_big grows the huge ones, one
+//                 block each
 //   k_resolve     a candidate wins when it holds the minimum claim on all its
 //                 cavity tets
 //   k_shared      two winners whose cavities share a face both stay only if
@@ -25,14 +35,17 @@
 //                 one steps back -- this exact test replaces a blanket
 //                 exclusion of neighbouring cavities
 //   k_alloc       recycled / fresh slots for the new tets
-//   k_write       new tets written, adjacency stitched by rotating around
-//                 boundary edges, cavity retired
+//   k_write       new tets written, adjacency stitched through an edge table
+//                 (rotation around boundary edges for the very largest
+//                 cavities), cavity retired
 //   k_relocate    points whose tet was retired walk (exact orient3d) from a
 //                 tet of the inserting point; the rest keep their tet; the
 //                 uninserted list is compacted with warp-aggregated appends
-// Strata: points are Morton-sorted per cloud (counting sort) and inserted in
-// the reference's stratified stride order (src/gpu/mod.rs:533-600), each new
-// stratum located by a walk from its predecessor on the curve.
+//   k_carry, k_end  recycled-slot carry-over, list swap, stop conditions
+// Strata: points are bucketed per cloud along a Morton (or Hilbert) curve
+// (counting sort) and inserted in the reference's stratified stride order
+// (src/gpu/mod.rs:533-600), each new stratum located by a walk from its
+// predecessor on the curve.
 #include <cuda_runtime.h>
 
 #include <algorithm>
