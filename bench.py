@@ -336,7 +336,7 @@ def run_gpu(args):
         },
         "clocks": clocks.summary(),
     }
-    if rank == 0 and not args.no_cpu_baseline and len(clouds) == 1:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and len(clouds) == 1:
         result["cpu_baseline"] = cpu_baseline(clouds[0], args.cpu_sample)
     if world == 1 and args.variants and args.workload == "mixture8M" and args.vote == "plain":
         result["variants"] = variants(wt, args)
