@@ -337,7 +337,8 @@ def delaunay(points, config: Config | None = None) -> DelaunayResult:
     if rc != WTET_OK:
         _raise(rc)
     k = m.value
-    return DelaunayResult(tets[:k].copy(), adj[:k].copy(), failed[: st.num_failed].copy(), st.as_dict())
+    # views of the output buffers: no second host copy of a multi-GB result
+    return DelaunayResult(tets[:k], adj[:k], failed[: st.num_failed].copy(), st.as_dict())
 
 
 def delaunay_batched(clouds, config: Config | None = None):
