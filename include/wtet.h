@@ -74,7 +74,11 @@ typedef struct wtet_config {
   uint32_t deep_threshold;         /* learned scheduler: a vote winner whose predicted probability
                                       of a large cavity exceeds deep_threshold/256 pre-claims two
                                       rings of neighbours; 0 = default (64, i.e. 1/4) */
-  uint32_t reserved[2];
+  uint32_t initial_capacity;       /* initial tet slots per point, in eighths; 0 = default (72, i.e. 9
+                                      per point).  When a round runs out of slots the tet arrays grow
+                                      in place by half (stats.capacity_grows counts it); small values
+                                      force that path.  Never changes the result. */
+  uint32_t reserved[1];
 } wtet_config;
 
 /* Per-call statistics (the reference prints these as [DEBUG]/[TIMING] lines,
@@ -92,6 +96,7 @@ typedef struct wtet_stats {
   uint64_t kernel_launches;   /* CUDA kernels executed by the call (graph nodes included) */
   double device_ms;           /* device time of the call, CUDA events */
   uint64_t vote_winners;      /* points that won their tet's vote (insertion attempts) */
+  uint64_t capacity_grows;    /* times the tet arrays grew during the run */
 } wtet_stats;
 
 /* Host-memory result owned by the library; release with wtet_result_free. */
@@ -148,19 +153,62 @@ int wtet_delaunay_batched(const float* xyz, const uint64_t* offsets, uint32_t nu
 int wtet_check_quality(const float* xyz, uint64_t n, const uint32_t* tets, const uint32_t* adjacency,
                        uint64_t m, uint64_t* violations, uint64_t* interior_tets);
 
+/* Every-face exact verification (extends check_delaunay_quality,
+ * src/lib.rs:25-78, which tests only faces between two all-real tets): every
+ * face between two tets that do not use the infinity vertex n+4 -- faces with
+ * super vertices included, at the reference's super coordinates
+ * (src/gpu/mod.rs:151-158) -- is tested with exact orient4d + SoS; every such
+ * tet with exact orient3d + SoS (it must be +1, src/phase2.rs:404-410); every
+ * adjacency link for symmetry and for sharing its face.  A complete output
+ * passes with violations = misoriented = broken_links = bad_vertex_ids = 0 and
+ * hull_faces = 4 (the super tetrahedron's faces, which border infinity tets):
+ * it is then the Delaunay triangulation of the points plus the super vertices. */
+typedef struct wtet_verify_report {
+  uint64_t finite_tets;     /* tets without the infinity vertex */
+  uint64_t faces_checked;   /* faces between two finite tets, each counted once */
+  uint64_t violations;      /* of those: opposite vertex inside the circumsphere (orient4d < 0) */
+  uint64_t misoriented;     /* finite tets with orient3d_sos != +1 */
+  uint64_t broken_links;    /* links out of range, not symmetric, or not sharing the face */
+  uint64_t hull_faces;      /* faces of finite tets with no finite neighbour */
+  uint64_t bad_vertex_ids;  /* tets naming a vertex beyond n+4 */
+} wtet_verify_report;
+
+/* Host buffers (xyz n x 3 f32; tets, adjacency m x 4 u32). */
+int wtet_verify(const float* xyz, uint64_t n, const uint32_t* tets, const uint32_t* adjacency, uint64_t m,
+                wtet_verify_report* report);
+/* Device pointers on the current device; runs on `stream` (cudaStream_t as
+ * void*, NULL = default) and returns when the report is ready. */
+int wtet_verify_device(const float* d_xyz, uint64_t n, const uint32_t* d_tets, const uint32_t* d_adjacency,
+                       uint64_t m, wtet_verify_report* report, void* stream);
+
+/* Canonical parity form (the sorted-vertex form in which two outputs compare
+ * byte for byte; python.rs:282-341 / lib.rs:25-78 consume the reference's
+ * unsorted rows): the tets without the infinity vertex n+4, vertex ids sorted
+ * ascending in each row, rows sorted lexicographically; out_adjacency[4*i+s] =
+ * (canonical index of the neighbour across the face opposite sorted slot s << 5)
+ * | (sorted slot of the neighbour's opposite vertex), or WTET_INVALID towards a
+ * missing or infinity neighbour.  out_tets / out_adjacency need room for m rows;
+ * *num_rows receives the canonical row count. */
+int wtet_canonicalize(const uint32_t* tets, const uint32_t* adjacency, uint64_t m, uint64_t n, uint32_t* out_tets,
+                      uint32_t* out_adjacency, uint64_t* num_rows);
+/* Same on device pointers of the current device, on `stream`. */
+int wtet_canonicalize_device(const uint32_t* d_tets, const uint32_t* d_adjacency, uint64_t m, uint64_t n,
+                             uint32_t* d_out_tets, uint32_t* d_out_adjacency, uint64_t* num_rows, void* stream);
+
 /* Allocation-free exact quality check.  No counterpart in the reference.
- * For callers that must not allocate GPU memory during the call -- code that is
- * recording a CUDA stream capture, serving loops that cannot stall on or
- * fragment an allocator another framework owns, fixed memory budgets.  Same
- * result as wtet_check_quality, but d_xyz (n x 3 f32), d_tets and d_adjacency
- * (m x 4 u32) are device pointers and the scratch (normalised points, box,
- * counters) is a fixed 16 MiB array in device memory that each GPU holds while
- * the library is loaded.  n may not exceed WTET_NOALLOC_MAX_POINTS (larger n
- * returns WTET_ERR_ARG).  The first call on a device looks up that array's
- * address, so make it before any stream capture.  Calls share the array:
- * calls that overlap on the GPU race and must be serialised by the caller.
- * Runs on `stream` (cudaStream_t as void*, NULL = default) and returns when the
- * counts are ready. */
+ * For callers that cannot allocate GPU memory during the call: serving loops
+ * whose GPU memory belongs to an allocator another framework owns (a
+ * cudaMalloc from here would stall on, or fragment, that pool) and hosts whose
+ * memory budget is fixed up front.  Same result as wtet_check_quality, but
+ * d_xyz (n x 3 f32), d_tets and d_adjacency (m x 4 u32) are device pointers
+ * and the scratch (normalised points, box, counters) is a fixed 16 MiB array
+ * in device memory that each GPU holds while the library is loaded.  n may not
+ * exceed WTET_NOALLOC_MAX_POINTS (larger n returns WTET_ERR_ARG).  The first
+ * call on a device (and the first after that device's context was reset)
+ * looks up that array's address, so make it before any stream capture.  Calls
+ * share the array: calls that overlap on the GPU race and must be serialised
+ * by the caller.  Runs on `stream` (cudaStream_t as void*, NULL = default) and
+ * returns when the counts are ready. */
 #define WTET_NOALLOC_MAX_POINTS 1048576ull
 int wtet_check_quality_noalloc(const float* d_xyz, uint64_t n, const uint32_t* d_tets,
                                const uint32_t* d_adjacency, uint64_t m, uint64_t* violations,

@@ -58,10 +58,17 @@ class OracleStats(ctypes.Structure):
 
 
 def build(force: bool = False) -> str:
-    """Compile liboracle.so with the Makefile beside this file."""
-    if force or not os.path.exists(_LIB_PATH):
+    """Compile liboracle.so with the Makefile beside this file (make skips the
+    work when the library is newer than its sources)."""
+    if force or not os.path.exists(_LIB_PATH) or _stale():
         subprocess.run(["make", "-s", "-C", _HERE] + (["-B"] if force else []), check=True)
     return _LIB_PATH
+
+
+def _stale() -> bool:
+    t = os.path.getmtime(_LIB_PATH)
+    srcs = [f for f in os.listdir(_HERE) if f.endswith((".cpp", ".hpp", ".h"))]
+    return any(os.path.getmtime(os.path.join(_HERE, f)) > t for f in srcs)
 
 
 def lib():
@@ -105,6 +112,8 @@ def lib():
             f = getattr(L, name)
             f.restype = ctypes.c_int64
             f.argtypes = [P, ctypes.c_uint64, P, P, ctypes.c_uint64]
+        L.oracle_canonical.restype = ctypes.c_uint64
+        L.oracle_canonical.argtypes = [P, P, ctypes.c_uint64, ctypes.c_uint32, P, P]
         L.oracle_check_orientation.restype = ctypes.c_int64
         L.oracle_check_orientation.argtypes = [P, ctypes.c_uint64, P, ctypes.c_uint64]
         _lib = L
@@ -241,6 +250,30 @@ def check_orientation(points, tets) -> int:
 
 
 def canonical(tets, adj, n: int):
+    """Canonical parity form (C++, canon.cpp); same result as canonical_numpy."""
+    t = np.ascontiguousarray(tets, np.uint32).reshape(-1, 4)
+    a = np.ascontiguousarray(adj, np.uint32).reshape(-1, 4)
+    m = t.shape[0]
+    ot = np.empty((m, 4), np.uint32)
+    oa = np.empty((m, 4), np.uint32)
+    k = int(lib().oracle_canonical(_ptr(t), _ptr(a), m, n, _ptr(ot), _ptr(oa)))
+    ot.resize((k, 4), refcheck=False)
+    oa.resize((k, 4), refcheck=False)
+    return ot, oa
+
+
+def digest(canon_tets, canon_adj) -> str:
+    """SHA-256 of a canonical form: the tets' bytes, then the adjacency's
+    (little-endian u32)."""
+    import hashlib
+
+    h = hashlib.sha256()
+    h.update(np.ascontiguousarray(canon_tets, "<u4").tobytes())
+    h.update(np.ascontiguousarray(canon_adj, "<u4").tobytes())
+    return h.hexdigest()
+
+
+def canonical_numpy(tets, adj, n: int):
     """Canonical parity form.
 
     T_all: every tet without the infinity vertex n+4, vertex ids sorted, rows

@@ -78,6 +78,13 @@ int64_t oracle_check_delaunay_quality(const float* xyz, uint64_t n, const uint32
  * orient3d_sos == +1.  Returns the violation count, or -1 on a structural error. */
 int64_t oracle_check_local_delaunay(const float* xyz, uint64_t n, const uint32_t* tets,
                                     const uint32_t* adj, uint64_t m);
+/* Canonical parity form (canon.cpp): tets without the infinity vertex n+4,
+ * ids sorted in each row, rows sorted; adjacency re-indexed to that order
+ * (neighbour << 5 | sorted slot of its opposite vertex), INVALID towards a
+ * missing or infinity neighbour.  out_tets / out_adj need room for m rows;
+ * returns the number of canonical rows. */
+uint64_t oracle_canonical(const uint32_t* tets, const uint32_t* adj, uint64_t m, uint32_t n,
+                          uint32_t* out_tets, uint32_t* out_adj);
 /* Count of tets (without the infinity vertex) whose orient3d_sos != +1. */
 int64_t oracle_check_orientation(const float* xyz, uint64_t n, const uint32_t* tets, uint64_t m);
 

@@ -173,3 +173,26 @@ def test_full_size_batched(gpu):
         check_adjacency(r.tets, r.adjacency)
         single = gpu.delaunay(clouds[i])
         assert tet_set_digest(single.tets) == tet_set_digest(r.tets), i
+
+
+@pytest.mark.parametrize("name,make", [
+    ("uniform100k", lambda: fx.uniform(100_000, 1)),
+    ("lattice24", lambda: fx.lattice(24)),
+])
+def test_capacity_growth_matches_oracle(gpu, oracle_mod, name, make):
+    """Starting at one tet slot per point forces the in-place growth of the
+    tet arrays (recaptured round graph, displaced winners retried) several
+    times; the output is still the oracle's."""
+    r = assert_parity(gpu, oracle_mod, make(), gpu.Config(initial_capacity=8))
+    assert r.stats["capacity_grows"] >= 2, r.stats
+
+
+def test_capacity_growth_batched(gpu, oracle_mod):
+    clouds = fx.batched_clouds(16, 11, lo=64, hi=20000)
+    res = gpu.delaunay_batched(clouds, gpu.Config(initial_capacity=8))
+    assert res[0].stats["capacity_grows"] >= 2
+    for pts, r in zip(clouds, res):
+        tets, adj, _ = oracle_mod.delaunay(pts, 1)
+        gt, ga = oracle_mod.canonical(r.tets, r.adjacency, len(pts))
+        ot, oa = oracle_mod.canonical(tets, adj, len(pts))
+        assert np.array_equal(gt, ot) and np.array_equal(ga, oa)

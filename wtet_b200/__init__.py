@@ -20,6 +20,9 @@ from ._core import (  # noqa: F401
     Config,
     DelaunayResult,
     __version__,
+    canonical,
+    canonical_device,
+    canonical_digest,
     check_quality,
     decode_adjacency,
     delaunay,
@@ -28,6 +31,8 @@ from ._core import (  # noqa: F401
     encode_adjacency,
     gpu_info,
     initialize_gpu,
+    verify,
+    verify_device,
 )
 
 __all__ = [
@@ -37,6 +42,11 @@ __all__ = [
     "Config",
     "DelaunayResult",
     "check_quality",
+    "verify",
+    "verify_device",
+    "canonical",
+    "canonical_device",
+    "canonical_digest",
     "decode_adjacency",
     "encode_adjacency",
     "initialize_gpu",

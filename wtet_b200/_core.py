@@ -42,7 +42,8 @@ class _Config(ctypes.Structure):
         ("candidate_filter", ctypes.c_uint32),
         ("pool_factor", ctypes.c_uint32),
         ("deep_threshold", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 2),
+        ("initial_capacity", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 1),
     ]
 
 
@@ -60,6 +61,7 @@ class Stats(ctypes.Structure):
         ("kernel_launches", ctypes.c_uint64),
         ("device_ms", ctypes.c_double),
         ("vote_winners", ctypes.c_uint64),
+        ("capacity_grows", ctypes.c_uint64),
     ]
 
     def as_dict(self):
@@ -102,7 +104,26 @@ EXPORTS = (
     "wtet_autotune_resolve",
     "wtet_morton_index",
     "wtet_hilbert_index",
+    "wtet_verify",
+    "wtet_verify_device",
+    "wtet_canonicalize",
+    "wtet_canonicalize_device",
 )
+
+
+class VerifyReport(ctypes.Structure):
+    _fields_ = [
+        ("finite_tets", ctypes.c_uint64),
+        ("faces_checked", ctypes.c_uint64),
+        ("violations", ctypes.c_uint64),
+        ("misoriented", ctypes.c_uint64),
+        ("broken_links", ctypes.c_uint64),
+        ("hull_faces", ctypes.c_uint64),
+        ("bad_vertex_ids", ctypes.c_uint64),
+    ]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
 
 
 class TrainConfig(ctypes.Structure):
@@ -182,6 +203,14 @@ def load():
     L.wtet_morton_index.restype = ctypes.c_uint32
     L.wtet_hilbert_index.argtypes = [ctypes.c_uint32] * 4
     L.wtet_hilbert_index.restype = ctypes.c_uint32
+    L.wtet_verify.argtypes = [P, u64, P, P, u64, ctypes.POINTER(VerifyReport)]
+    L.wtet_verify.restype = ctypes.c_int
+    L.wtet_verify_device.argtypes = [P, u64, P, P, u64, ctypes.POINTER(VerifyReport), P]
+    L.wtet_verify_device.restype = ctypes.c_int
+    L.wtet_canonicalize.argtypes = [P, P, u64, u64, P, P, ctypes.POINTER(u64)]
+    L.wtet_canonicalize.restype = ctypes.c_int
+    L.wtet_canonicalize_device.argtypes = [P, P, u64, u64, P, P, ctypes.POINTER(u64), P]
+    L.wtet_canonicalize_device.restype = ctypes.c_int
     _lib = L
     _install_packaged_table()
     return L
@@ -212,15 +241,17 @@ class Config:
     ``vote`` ("plain" or "learned") selects the insertion scheduler;
     ``block_size``, ``rounds_per_graph``, ``overlap_shift``,
     ``candidate_filter`` and ``pool_factor`` are performance knobs (0 = the
-    autotuner's value for the job's size, see wtet_b200.autotune).  No option
-    changes the resulting triangulation."""
+    autotuner's value for the job's size, see wtet_b200.autotune);
+    ``initial_capacity`` sets the initial tet slots per point in eighths (0 =
+    9 per point; smaller values exercise the in-place growth of the tet
+    arrays).  No option changes the resulting triangulation."""
 
     def __init__(self, insertion_rule: str = "circumcenter", enable_flipping: bool = True,
                  enable_sorting: bool = False, enable_hilbert_sorting: bool = False,
                  enable_splaying: bool = True, max_insert_iterations: int = 100,
                  max_flip_iterations: int = 10, vote: str = "plain", block_size: int = 0,
                  rounds_per_graph: int = 0, overlap_shift: int = 0, candidate_filter: int = 0,
-                 pool_factor: int = 0, deep_threshold: int = 0):
+                 pool_factor: int = 0, deep_threshold: int = 0, initial_capacity: int = 0):
         rule = str(insertion_rule).lower()
         if rule not in _RULES:
             raise ValueError(
@@ -242,6 +273,7 @@ class Config:
         self.candidate_filter = int(candidate_filter)
         self.pool_factor = int(pool_factor)
         self.deep_threshold = int(deep_threshold)
+        self.initial_capacity = int(initial_capacity)
 
     def _c(self) -> _Config:
         if self.vote == "learned":
@@ -261,6 +293,7 @@ class Config:
         c.candidate_filter = self.candidate_filter
         c.pool_factor = self.pool_factor
         c.deep_threshold = self.deep_threshold
+        c.initial_capacity = self.initial_capacity
         return c
 
     def __repr__(self) -> str:
@@ -337,8 +370,12 @@ def delaunay(points, config: Config | None = None) -> DelaunayResult:
     if rc != WTET_OK:
         _raise(rc)
     k = m.value
-    # views of the output buffers: no second host copy of a multi-GB result
-    return DelaunayResult(tets[:k], adj[:k], failed[: st.num_failed].copy(), st.as_dict())
+    # The buffers were sized for the worst case (8n + 64 rows, about 20% above
+    # a typical 6.7n): shrink them in place (realloc of the tail, no second
+    # multi-GB copy) so that the result holds only its own rows.
+    tets.resize((k, 4), refcheck=False)
+    adj.resize((k, 4), refcheck=False)
+    return DelaunayResult(tets, adj, failed[: st.num_failed].copy(), st.as_dict())
 
 
 def delaunay_batched(clouds, config: Config | None = None):
@@ -436,6 +473,86 @@ def check_quality(points, result: DelaunayResult):
     if rc != WTET_OK:
         _raise(rc)
     return int(v.value), int(i.value)
+
+
+def verify(points, result: DelaunayResult) -> dict:
+    """Every-face exact verification on the device (extends check_quality,
+    src/lib.rs:25-78, to faces with super vertices; checks orientation and
+    links too).  A complete output has violations = misoriented =
+    broken_links = bad_vertex_ids = 0 and hull_faces = 4."""
+    pts = _points(points)
+    t = np.ascontiguousarray(result.tets, np.uint32).reshape(-1, 4)
+    a = np.ascontiguousarray(result.adjacency, np.uint32).reshape(-1, 4)
+    rep = VerifyReport()
+    rc = load().wtet_verify(_ptr(pts), pts.shape[0], _ptr(t), _ptr(a), t.shape[0], ctypes.byref(rep))
+    if rc != WTET_OK:
+        _raise(rc)
+    return rep.as_dict()
+
+
+def verify_device(points, tets, adjacency) -> dict:
+    """verify() on CUDA torch tensors (points (N,3) f32; tets, adjacency
+    (M,4) 32-bit), on torch's current stream."""
+    import torch
+
+    rep = VerifyReport()
+    stream = ctypes.c_void_p(torch.cuda.current_stream(points.device).cuda_stream)
+    rc = load().wtet_verify_device(ctypes.c_void_p(points.data_ptr()), points.shape[0],
+                                   ctypes.c_void_p(tets.data_ptr()), ctypes.c_void_p(adjacency.data_ptr()),
+                                   tets.shape[0], ctypes.byref(rep), stream)
+    if rc != WTET_OK:
+        _raise(rc)
+    return rep.as_dict()
+
+
+def canonical(tets, adjacency, n: int):
+    """Canonical parity form, computed on the device: tets without the
+    infinity vertex n+4, ids sorted per row, rows sorted; adjacency re-indexed
+    to that order ((neighbour << 5) | sorted slot of its opposite vertex,
+    INVALID towards a missing or infinity neighbour).  Returns numpy
+    (K,4) uint32 arrays."""
+    t = np.ascontiguousarray(tets, np.uint32).reshape(-1, 4)
+    a = np.ascontiguousarray(adjacency, np.uint32).reshape(-1, 4)
+    m = t.shape[0]
+    ot = np.empty((max(m, 1), 4), np.uint32)
+    oa = np.empty((max(m, 1), 4), np.uint32)
+    k = ctypes.c_uint64(0)
+    rc = load().wtet_canonicalize(_ptr(t), _ptr(a), m, int(n), _ptr(ot), _ptr(oa), ctypes.byref(k))
+    if rc != WTET_OK:
+        _raise(rc)
+    ot.resize((k.value, 4), refcheck=False)
+    oa.resize((k.value, 4), refcheck=False)
+    return ot, oa
+
+
+def canonical_device(tets, adjacency, n: int):
+    """canonical() on CUDA torch tensors; returns CUDA tensors (K,4)."""
+    import torch
+
+    m = tets.shape[0]
+    ot = torch.empty((max(m, 1), 4), dtype=torch.int32, device=tets.device)
+    oa = torch.empty((max(m, 1), 4), dtype=torch.int32, device=tets.device)
+    k = ctypes.c_uint64(0)
+    stream = ctypes.c_void_p(torch.cuda.current_stream(tets.device).cuda_stream)
+    rc = load().wtet_canonicalize_device(ctypes.c_void_p(tets.data_ptr()), ctypes.c_void_p(adjacency.data_ptr()), m,
+                                         int(n), ctypes.c_void_p(ot.data_ptr()), ctypes.c_void_p(oa.data_ptr()),
+                                         ctypes.byref(k), stream)
+    if rc != WTET_OK:
+        _raise(rc)
+    return ot[: k.value], oa[: k.value]
+
+
+def canonical_digest(canon_tets, canon_adjacency) -> str:
+    """SHA-256 of a canonical form: the tets' bytes, then the adjacency's
+    (little-endian u32)."""
+    import hashlib
+
+    h = hashlib.sha256()
+    for arr in (canon_tets, canon_adjacency):
+        if hasattr(arr, "cpu"):
+            arr = arr.cpu().numpy()
+        h.update(np.ascontiguousarray(arr).view(np.uint32).astype("<u4", copy=False).tobytes())
+    return h.hexdigest()
 
 
 def decode_adjacency(packed: int):

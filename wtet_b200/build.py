@@ -15,8 +15,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libwtet.so")
-SOURCES = ["engine.cu", "capi.cu", "noalloc.cu", "learned.cu", "sort.cu"]
-HEADERS = ["exact.cuh", "engine.cuh", "learned.cuh", "order.cuh"]
+SOURCES = ["engine.cu", "capi.cu", "noalloc.cu", "learned.cu", "verify.cu"]
+HEADERS = ["exact.cuh", "engine.cuh", "learned.cuh", "order.cuh", "devbuf.cuh"]
 
 NVCC_FLAGS = [
     "-O3",

@@ -3,6 +3,7 @@
 // device, and turns engine errors into status codes and messages.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -236,6 +237,81 @@ int wtet_check_quality(const float* xyz, uint64_t n, const uint32_t* tets, const
       ck(cudaMemcpyAsync(d_a, adjacency, m * 16, cudaMemcpyHostToDevice, s), "copy adjacency");
     }
     wtet::check_quality_device(d_xyz, n, d_t, d_a, m, violations, interior_tets, s);
+    return WTET_OK;
+  } catch (const wtet::Error& e) {
+    return fail(e.status, e.msg);
+  }
+}
+
+int wtet_verify_device(const float* d_xyz, uint64_t n, const uint32_t* d_tets, const uint32_t* d_adjacency,
+                       uint64_t m, wtet_verify_report* report, void* stream) {
+  if (!d_xyz || !report || (m && (!d_tets || !d_adjacency))) return fail(WTET_ERR_ARG, "null pointer argument");
+  try {
+    require_device();
+    wtet::verify_device(d_xyz, n, d_tets, d_adjacency, m, report, static_cast<cudaStream_t>(stream));
+    return WTET_OK;
+  } catch (const wtet::Error& e) {
+    return fail(e.status, e.msg);
+  }
+}
+
+int wtet_verify(const float* xyz, uint64_t n, const uint32_t* tets, const uint32_t* adjacency, uint64_t m,
+                wtet_verify_report* report) {
+  if (!xyz || !report || (m && (!tets || !adjacency))) return fail(WTET_ERR_ARG, "null pointer argument");
+  try {
+    require_device();
+    cudaStream_t s = nullptr;
+    float* d_xyz = wtet::ws_input(3 * n + 8 * m + 8);
+    uint32_t* d_t = reinterpret_cast<uint32_t*>(d_xyz + 3 * n + ((4 - (3 * n) % 4) % 4));
+    uint32_t* d_a = d_t + 4 * m;
+    ck(cudaMemcpyAsync(d_xyz, xyz, 3 * n * 4, cudaMemcpyHostToDevice, s), "copy points");
+    if (m) {
+      ck(cudaMemcpyAsync(d_t, tets, m * 16, cudaMemcpyHostToDevice, s), "copy tets");
+      ck(cudaMemcpyAsync(d_a, adjacency, m * 16, cudaMemcpyHostToDevice, s), "copy adjacency");
+    }
+    wtet::verify_device(d_xyz, n, d_t, d_a, m, report, s);
+    return WTET_OK;
+  } catch (const wtet::Error& e) {
+    return fail(e.status, e.msg);
+  }
+}
+
+int wtet_canonicalize_device(const uint32_t* d_tets, const uint32_t* d_adjacency, uint64_t m, uint64_t n,
+                             uint32_t* d_out_tets, uint32_t* d_out_adjacency, uint64_t* num_rows, void* stream) {
+  if (!num_rows || (m && (!d_tets || !d_adjacency || !d_out_tets || !d_out_adjacency)))
+    return fail(WTET_ERR_ARG, "null pointer argument");
+  try {
+    require_device();
+    *num_rows = wtet::canonicalize_device(d_tets, d_adjacency, m, n, d_out_tets, d_out_adjacency,
+                                          static_cast<cudaStream_t>(stream));
+    return WTET_OK;
+  } catch (const wtet::Error& e) {
+    return fail(e.status, e.msg);
+  }
+}
+
+int wtet_canonicalize(const uint32_t* tets, const uint32_t* adjacency, uint64_t m, uint64_t n, uint32_t* out_tets,
+                      uint32_t* out_adjacency, uint64_t* num_rows) {
+  if (!num_rows || (m && (!tets || !adjacency || !out_tets || !out_adjacency)))
+    return fail(WTET_ERR_ARG, "null pointer argument");
+  try {
+    require_device();
+    cudaStream_t s = nullptr;
+    // inputs in the per-thread input buffer, outputs in the output buffers
+    uint32_t* d_in = reinterpret_cast<uint32_t*>(wtet::ws_input(8 * m + 4));
+    uint32_t *d_ot = nullptr, *d_oa = nullptr;
+    wtet::ws_outputs(std::max<uint64_t>(m, 1), &d_ot, &d_oa);
+    if (m) {
+      ck(cudaMemcpyAsync(d_in, tets, m * 16, cudaMemcpyHostToDevice, s), "copy tets");
+      ck(cudaMemcpyAsync(d_in + 4 * m, adjacency, m * 16, cudaMemcpyHostToDevice, s), "copy adjacency");
+    }
+    const uint64_t k = wtet::canonicalize_device(d_in, d_in + 4 * m, m, n, d_ot, d_oa, s);
+    *num_rows = k;
+    if (k) {
+      ck(cudaMemcpyAsync(out_tets, d_ot, k * 16, cudaMemcpyDeviceToHost, s), "copy canonical tets");
+      ck(cudaMemcpyAsync(out_adjacency, d_oa, k * 16, cudaMemcpyDeviceToHost, s), "copy canonical adjacency");
+    }
+    ck(cudaStreamSynchronize(s), "synchronize");
     return WTET_OK;
   } catch (const wtet::Error& e) {
     return fail(e.status, e.msg);

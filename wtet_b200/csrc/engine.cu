@@ -60,6 +60,7 @@
 #include "exact.cuh"
 #include "learned.cuh"
 #include "order.cuh"
+#include "devbuf.cuh"
 
 namespace wtet {
 
@@ -1691,107 +1692,13 @@ __global__ void k_infinity(Dev D, const CloudInfo* ci, uint32_t nc, const uint32
   }
 }
 
-// ----------------------------------------------------------- scan utils ----
-
-__global__ void k_scan_blocks(const uint32_t* in, uint32_t* out, uint32_t* sums, uint32_t n) {
-  __shared__ uint32_t warp_tot[32];
-  const uint32_t per = 4;
-  uint32_t base = blockIdx.x * blockDim.x * per;
-  uint32_t v[per];
-  uint32_t local = 0;
-  for (uint32_t k = 0; k < per; ++k) {
-    uint32_t i = base + threadIdx.x * per + k;
-    v[k] = i < n ? in[i] : 0u;
-    local += v[k];
-  }
-  uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint32_t x = local;
-  for (int o = 1; o < 32; o <<= 1) {
-    uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
-    if (lane >= uint32_t(o)) x += y;
-  }
-  if (lane == 31) warp_tot[warp] = x;
-  __syncthreads();
-  if (warp == 0) {
-    uint32_t w = lane < (blockDim.x >> 5) ? warp_tot[lane] : 0u;
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
-      if (lane >= uint32_t(o)) w += y;
-    }
-    warp_tot[lane] = w;
-  }
-  __syncthreads();
-  uint32_t excl = x - local + (warp ? warp_tot[warp - 1] : 0u);
-  for (uint32_t k = 0; k < per; ++k) {
-    uint32_t i = base + threadIdx.x * per + k;
-    if (i < n) out[i] = excl;
-    excl += v[k];
-  }
-  if (threadIdx.x == blockDim.x - 1) sums[blockIdx.x] = excl;
-}
-
-__global__ void k_scan_add(uint32_t* out, const uint32_t* sums, uint32_t n) {
-  uint32_t base = blockIdx.x * blockDim.x * 4;
-  uint32_t add = sums[blockIdx.x];
-  for (uint32_t k = 0; k < 4; ++k) {
-    uint32_t i = base + threadIdx.x * 4 + k;
-    if (i < n) out[i] += add;
-  }
-}
-
 // ------------------------------------------------------------- host side ----
 
+using dev::ck;
+using dev::DBuf;
+using dev::scan_u32;
+
 namespace {
-
-void ck(cudaError_t e, const char* what) {
-  if (e != cudaSuccess) throw Error{WTET_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
-}
-
-template <class T>
-struct DBuf {
-  T* p = nullptr;
-  size_t n = 0;
-  void reserve(size_t want, const char* what) {
-    if (want <= n) return;
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-    ck(cudaMalloc(&p, std::max<size_t>(want, 1) * sizeof(T)), what);
-    n = want;
-  }
-  void grow_keep(size_t want, size_t used, cudaStream_t s, const char* what) {
-    if (want <= n) return;
-    T* q = nullptr;
-    ck(cudaMalloc(&q, want * sizeof(T)), what);
-    if (p && used) ck(cudaMemcpyAsync(q, p, used * sizeof(T), cudaMemcpyDeviceToDevice, s), what);
-    ck(cudaStreamSynchronize(s), what);
-    if (p) cudaFree(p);
-    p = q;
-    n = want;
-  }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-  }
-};
-
-// Exclusive scan in place over n u32 (recursive over block sums).
-int scan_u32(uint32_t* d, uint32_t n, cudaStream_t s, std::vector<DBuf<uint32_t>>& tmp, int depth = 0) {
-  if (n == 0) return 0;
-  const uint32_t threads = 256, per_block = threads * 4;
-  uint32_t blocks = (n + per_block - 1) / per_block;
-  if (int(tmp.size()) <= depth) tmp.resize(depth + 1);
-  tmp[depth].reserve(size_t(blocks) + 1, "scan sums");
-  k_scan_blocks<<<blocks, threads, 0, s>>>(d, d, tmp[depth].p, n);
-  int launches = 1;
-  if (blocks > 1) {
-    launches += scan_u32(tmp[depth].p, blocks, s, tmp, depth + 1);
-    k_scan_add<<<blocks, threads, 0, s>>>(d, tmp[depth].p, n);
-    ++launches;
-  }
-  return launches;
-}
 
 uint32_t initial_stride_log2(uint64_t n) {
   // src/gpu/mod.rs:533-548
@@ -2117,7 +2024,8 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   }
   const uint64_t nv = n + 4ull * nc;
   uint64_t cap0 = 0;
-  for (uint32_t c = 0; c < nc; ++c) cap0 += uint64_t(ci[c].n) * 9 / 2 * 2 + 64;  // ~9 n
+  const uint64_t slots_x8 = job.cfg.initial_capacity ? std::min<uint32_t>(job.cfg.initial_capacity, 1024u) : 72u;
+  for (uint32_t c = 0; c < nc; ++c) cap0 += uint64_t(ci[c].n) * slots_x8 / 8 + 64;  // 9 n by default
   cap0 = std::min<uint64_t>(cap0, 0x7FFFFFF0ull);
 
   W.off.reserve(nc + 1, "offsets");
@@ -2398,6 +2306,7 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
         ck(cudaMemsetAsync(W.tcount.p, 0, ncap * 4, s), "memset");
       }
       cap = ncap;
+      st.capacity_grows += 1;
       refresh();
       hs.stop = 0;
       ck(cudaMemcpyAsync(W.state.p, &hs, sizeof(State), cudaMemcpyHostToDevice, s), "h2d");
@@ -2519,6 +2428,38 @@ __global__ void k_normalize_plain(const float* xyz, uint64_t n, const uint32_t* 
   float s = fmaxf(fmaxf(fmaxf(ext[0], ext[1]), ext[2]), 1e-10f);
   out[i] = make_float4(__fdiv_rn(__fsub_rn(xyz[3 * i], lo[0]), s), __fdiv_rn(__fsub_rn(xyz[3 * i + 1], lo[1]), s),
                        __fdiv_rn(__fsub_rn(xyz[3 * i + 2], lo[2]), s), 0.f);
+}
+
+// Single-cloud normalisation without the engine's workspace: the box is
+// reduced with an offsets-free variant of k_bbox.
+__global__ void k_bbox_one(const float* xyz, uint64_t n, uint32_t* mn, uint32_t* mx) {
+  __shared__ uint32_t smn[3], smx[3];
+  if (threadIdx.x < 3) {
+    smn[threadIdx.x] = 0xFFFFFFFFu;
+    smx[threadIdx.x] = 0u;
+  }
+  __syncthreads();
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+    for (int k = 0; k < 3; ++k) {
+      const float v = xyz[3 * i + k];
+      if (v != v) continue;  // NaN is ignored, as f32::min / f32::max do
+      atomicMin(&smn[k], f2o(v));
+      atomicMax(&smx[k], f2o(v));
+    }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    atomicMin(&mn[threadIdx.x], smn[threadIdx.x]);
+    atomicMax(&mx[threadIdx.x], smx[threadIdx.x]);
+  }
+}
+
+void normalize_points_device(const float* d_xyz, uint64_t n, float4* d_out, uint32_t* box, cudaStream_t s) {
+  ck(cudaMemsetAsync(box, 0xFF, 12, s), "memset");
+  ck(cudaMemsetAsync(box + 3, 0x00, 12, s), "memset");
+  if (n == 0) return;
+  k_bbox_one<<<blocks_for(n, 256, 148 * 4), 256, 0, s>>>(d_xyz, n, box, box + 3);
+  k_normalize_plain<<<uint32_t((n + 255) / 256), 256, 0, s>>>(d_xyz, n, box, box + 3, d_out);
+  ck(cudaGetLastError(), "normalise kernels");
 }
 
 void check_quality_device(const float* d_xyz, uint64_t n, const uint32_t* d_tets, const uint32_t* d_adj, uint64_t m,

@@ -55,6 +55,19 @@ JobResult run_job(const Job& job, uint32_t* d_tets, uint32_t* d_adj, uint64_t ca
 void check_quality_device(const float* d_xyz, uint64_t n, const uint32_t* d_tets, const uint32_t* d_adj,
                           uint64_t m, uint64_t* violations, uint64_t* interior, cudaStream_t stream);
 
+// Normalised points (src/lib.rs:313-337) of one cloud into d_out (n float4,
+// w = 0); box is scratch for 6 u32 (ordered min / max per axis).
+void normalize_points_device(const float* d_xyz, uint64_t n, float4* d_out, uint32_t* box, cudaStream_t stream);
+
+// Every-face exact verification of a triangulation (verify.cu).
+void verify_device(const float* d_xyz, uint64_t n, const uint32_t* d_tets, const uint32_t* d_adj, uint64_t m,
+                   wtet_verify_report* report, cudaStream_t stream);
+
+// Canonical parity form on the device (verify.cu); returns the row count.
+uint64_t canonicalize_device(const uint32_t* d_tets, const uint32_t* d_adj, uint64_t m, uint64_t n,
+                             uint32_t* d_out_tets, uint32_t* d_out_adj, cudaStream_t stream);
+void release_verify_workspace();
+
 // Upper bound on output tets for a cloud of n points.
 uint64_t max_tets_for(uint64_t n);
 

@@ -1,14 +1,13 @@
 // Allocation-free variant of the exact quality check (wtet_check_quality).
 //
-// Some callers cannot allocate GPU memory while they run this check: code
-// that is recording a CUDA stream capture (a cudaMalloc there breaks the
-// capture), serving loops that must not stall on the allocator or fragment
-// a memory pool that another framework owns, and hosts whose memory budget
-// is fixed up front.  This entry point therefore keeps its scratch -- the
-// normalised points, the bounding box and the counters -- in one file-scope
-// device array of fixed size, which every GPU that loads libwtet.so holds
-// until the process exits.  It calls no cudaMalloc, cudaFree or allocating
-// library routine.
+// Some callers cannot allocate GPU memory while they run this check: serving
+// loops whose GPU memory belongs to an allocator that another framework owns
+// (a cudaMalloc from the library would stall on, or fragment, that pool), and
+// hosts whose memory budget is fixed up front so that no call may grow it.
+// This entry point therefore keeps its scratch -- the normalised points, the
+// bounding box and the counters -- in one file-scope device array of fixed
+// size, which every GPU that loads libwtet.so holds until the process exits.
+// It calls no cudaMalloc, cudaFree or allocating library routine.
 //
 // The array is shared by every call on a device and keeps the last call's
 // contents; each call clears the parts that must start at zero.  Calls whose
@@ -132,11 +131,48 @@ __global__ void k_check(uint64_t n, const uint4* tets, const uint4* adj, uint64_
   atomicAdd(&cnt[1], interior);
 }
 
-std::mutex g_mu;
-void* g_ptr[64] = {};
+// The device address of g_scratch belongs to the context the module was
+// loaded into: after cudaDeviceReset the primary context is created anew and
+// the array may move.  The cache is therefore keyed on the context's unique
+// id (cuCtxGetId, reached through the runtime's driver entry points so that
+// the library needs no link against libcuda).
+typedef int (*CtxGetCurrentFn)(void**);
+typedef int (*CtxGetIdFn)(void*, unsigned long long*);
 
-// Device address of g_scratch for the current device, looked up once per
-// device with that device current (host code must not use &g_scratch).
+struct ScratchEntry {
+  unsigned long long ctx_id = 0;
+  void* ptr = nullptr;
+};
+
+std::mutex g_mu;
+ScratchEntry g_cache[64];
+
+// Unique id of the current context (0 when it cannot be read).
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+    looked_up = true;
+  }
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current && get_id && get_current(&ctx) == 0 && ctx && get_id(ctx, &id) == 0) return id;
+  return 0;
+}
+
+// Device address of g_scratch in the current device's context, looked up once
+// per context with that device current (host code must not use &g_scratch:
+// in host code that name is a host-side stand-in, not a device address).
 int scratch_for_current_device(unsigned char** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -144,17 +180,27 @@ int scratch_for_current_device(unsigned char** out) {
     wtet::set_last_error("no usable CUDA device");
     return WTET_ERR_CUDA;
   }
+  // cudaSetDevice creates the device's primary context (CUDA 12), so that its
+  // id can be read before the first launch.
+  e = cudaSetDevice(dev);
+  if (e != cudaSuccess) {
+    wtet::set_last_error(std::string("no usable CUDA context: ") + cudaGetErrorString(e));
+    return WTET_ERR_CUDA;
+  }
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_ptr[dev]) {
+  const unsigned long long ctx = current_context_id();
+  ScratchEntry& c = g_cache[dev];
+  if (!c.ptr || ctx == 0 || c.ctx_id != ctx) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_scratch);
     if (e != cudaSuccess || !p) {
       wtet::set_last_error(std::string("cudaGetSymbolAddress(scratch) failed: ") + cudaGetErrorString(e));
       return WTET_ERR_CUDA;
     }
-    g_ptr[dev] = p;
+    c.ptr = p;
+    c.ctx_id = ctx;
   }
-  *out = static_cast<unsigned char*>(g_ptr[dev]);
+  *out = static_cast<unsigned char*>(c.ptr);
   return WTET_OK;
 }
 
@@ -178,6 +224,14 @@ int wtet_check_quality_noalloc(const float* d_xyz, uint64_t n, const uint32_t* d
   unsigned char* scratch = nullptr;
   int rc = scratch_for_current_device(&scratch);
   if (rc != WTET_OK) return rc;
+  // An error left pending by the caller's own earlier work is neither taken
+  // (cleared) nor reported as this call's: the call refuses to run instead.
+  cudaError_t prior = cudaPeekAtLastError();
+  if (prior != cudaSuccess) {
+    wtet::set_last_error(std::string("a CUDA error from earlier work on this thread is pending: ") +
+                         cudaGetErrorString(prior));
+    return WTET_ERR_CUDA;
+  }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   // Only the box, the counters and the error word must start cleared.
   cudaError_t e = cudaMemsetAsync(scratch + kBoxOff, 0xFF, 12, s);
