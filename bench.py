@@ -15,13 +15,14 @@ compaction).  `--workload batched` runs 4,096 clouds of log-uniform sizes in
   roofline  algorithmic bytes 12 B/point + 32 B/tet per triangulation over its
             device time, against the measured HBM copy bandwidth
   cpu_baseline  the oracle (sequential exact Bowyer-Watson restating the
-            reference's CPU path) on a bounded sample, 1 core
+            reference's CPU path) on the whole workload, 1 core; its canonical
+            output is compared with the GPU's (parity)
 
 Multi-GPU: a single cloud does not shard, so N ranks run N replicas (weak
 scaling); the batched workload splits its clouds across ranks.
 `--impl reference` times the reference's CPU algorithm (the oracle port; the
 Rust/wgpu reference cannot be built or run on this machine) with all host
-cores on the same metric.
+cores on the same workload and metric: each step one complete triangulation.
 """
 from __future__ import annotations
 
@@ -161,12 +162,35 @@ def max_over_ranks(x: float, world: int) -> float:
     return reduce_over_ranks(x, world, "max")
 
 
+def cloud_cost(n: int) -> float:
+    """Estimated work of one cloud: n log n (point location and the rounds
+    of a cloud grow like that)."""
+    return float(n) * np.log2(max(int(n), 2))
+
+
+def lpt_assign(sizes, world: int):
+    """Longest-processing-time-first assignment of clouds to ranks: clouds in
+    decreasing estimated cost, each to the rank with the least work so far.
+    Returns the rank of every cloud (deterministic: ties go to the lower
+    rank, equal costs keep their input order)."""
+    order = sorted(range(len(sizes)), key=lambda i: (-cloud_cost(sizes[i]), i))
+    load = [0.0] * world
+    owner = [0] * len(sizes)
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        owner[i] = r
+        load[r] += cloud_cost(sizes[i])
+    return owner
+
+
 def shard(clouds, rank: int, world: int):
-    """Clouds of a batched workload owned by one rank (round robin); a
-    single cloud is not split -- every rank runs a replica."""
-    if len(clouds) == 1:
+    """Clouds of a batched workload owned by one rank (LPT over the n log n
+    cost estimate, input order kept inside a rank); a single cloud is not
+    split -- every rank runs a replica."""
+    if len(clouds) == 1 or world == 1:
         return clouds
-    return clouds[rank::world]
+    owner = lpt_assign([len(c) for c in clouds], world)
+    return [c for c, o in zip(clouds, owner) if o == rank]
 
 
 def barrier(world):
@@ -174,6 +198,26 @@ def barrier(world):
         import torch.distributed as dist
 
         dist.barrier()
+
+
+def bench_config(workload: str, vote: str, world: int):
+    """The workload description printed by both arms (identical dicts, so the
+    two lines are on the same configuration)."""
+    clouds = 1 if workload != "batched" else 4096
+    cfg = {
+        "workload": workload,
+        "description": WORKLOADS[workload],
+        "points": POINTS[workload],
+        "clouds": clouds,
+        "vote": vote,
+        "parallelism": "replicas (a single triangulation does not shard)" if clouds == 1
+        else "clouds split across ranks by LPT over n log n, no data-path collective",
+        "l2": "inputs larger than the 126 MB L2: tets, adjacency and claim arrays of several GB",
+    }
+    if workload == "batched":
+        cfg["batching"] = "all clouds in one job: insertion rounds over every cloud replayed from CUDA graphs " \
+                          "(graph nodes are the grid-wide barriers; no persistent kernel)"
+    return cfg
 
 
 def run_gpu(args):
@@ -309,15 +353,7 @@ def run_gpu(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {
-            "workload": args.workload,
-            "description": WORKLOADS[args.workload],
-            "points_per_rank": n_points,
-            "clouds_per_rank": len(clouds),
-            "vote": args.vote,
-            "parallelism": "replicas" if len(clouds) == 1 else "clouds split across ranks",
-            "l2": "working set (tets, adjacency, claims: several GB) larger than the 126 MB L2",
-        },
+        "config": bench_config(args.workload, args.vote, world),
         "e2e": e2e,
         "gpu_launches": int(launches),
         "rounds": int(rounds),
@@ -329,17 +365,25 @@ def run_gpu(args):
             "unit": "GB/s",
             "frac": round(achieved / hbm, 5),
             "traffic": TRAFFIC.get(args.workload),
-            "basis": "whole triangulation per step (about 3,000 launches of 13 round kernels replayed from CUDA "
-                     "graphs, so no single launch is the unit): 12 B/point read + 32 B/tet written over its "
-                     f"device time; peak = {peak_kind} copy bandwidth; traffic = DRAM bytes of one "
-                     "triangulation from ncu (1M mixture, scaled by points)",
+            "traffic_source": TRAFFIC_SOURCE if args.workload in TRAFFIC else None,
+            "basis": "whole triangulation per step (thousands of launches of the round kernels replayed from "
+                     "CUDA graphs, so no single launch is the unit): 12 B/point read + 32 B/tet written over its "
+                     f"device time; peak = {peak_kind} copy bandwidth; traffic = DRAM bytes read + written by all "
+                     "launches of one triangulation (ncu)",
         },
         "clocks": clocks.summary(),
     }
+    golden = golden_digests()
+    if len(clouds) == 1:
+        # the last step's output, canonical on the device, against the oracle's
+        gdig = device_digest(wt, d_t, d_a, num_tets, n_points)
+        gname = GOLDEN_NAME.get(args.workload)
+        result["parity"] = {"canonical_sha256": gdig,
+                            "same_as_stored_oracle_digest": bool(gname in golden and golden[gname]["sha256"] == gdig)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline and len(clouds) == 1:
-        result["cpu_baseline"] = cpu_baseline(clouds[0], args.cpu_sample)
+        result["cpu_baseline"] = cpu_baseline(clouds[0], result["parity"]["canonical_sha256"])
     if world == 1 and args.variants and args.workload == "mixture8M" and args.vote == "plain":
-        result["variants"] = variants(wt, args)
+        result["variants"] = variants(wt, args, golden)
     if rank == 0:
         print(json.dumps(result), flush=True)
     if world > 1:
@@ -348,17 +392,13 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
-# DRAM bytes (read + write) per triangulation, from an ncu launch list of one
-# triangulation of the 1M-point mixture (dram__bytes_read.sum +
-# dram__bytes_write.sum over all launches, --cache-control none), scaled by the
-# point count for the larger clouds of the same distribution
-# (profiles/launch_list_mixture1M.md).
-_TRAFFIC_1M_MIXTURE = 49.934e9
-TRAFFIC: dict = {
-    "mixture1M": _TRAFFIC_1M_MIXTURE,
-    "mixture8M": 8 * _TRAFFIC_1M_MIXTURE,
-    "mixture8M_new": 8 * _TRAFFIC_1M_MIXTURE,
-}
+# DRAM bytes (read + write) of one whole triangulation: ncu launch list of one
+# 8M-mixture triangulation with dram__bytes_read.sum + dram__bytes_write.sum
+# (a one-pass metric set, so every launch is captured unreplayed), summed over
+# all launches.  Measured on the kernels of the revision named beside it; a
+# kernel change needs a new capture (profiles/ holds the summary and command).
+TRAFFIC: dict = {}
+TRAFFIC_SOURCE = ""
 
 WORKLOADS = {
     "mixture8M": "8,000,000 points: 60% uniform [0,1]^3, 30% Gaussian ball (0.5, sigma 0.1), "
@@ -373,56 +413,95 @@ WORKLOADS = {
     "batched": "4,096 clouds, sizes log-uniform in [64, 65536], each uniform / Gaussian / shell / "
                "jittered lattice, float32, seed 4",
 }
+POINTS = {"mixture8M": 8_000_000, "uniform8M": 8_000_000, "mixture8M_new": 8_000_000, "mixture1M": 1_000_000,
+          "uniform100k": 100_000, "mixture100k": 100_000, "lattice2M": 128 ** 3, "sphere1M": 1_000_000,
+          "batched": 39_908_171}
+# workload -> entry of tests/golden/full_size.json (the oracle's canonical digest)
+GOLDEN_NAME = {"mixture8M": "mixture8M_s3", "mixture8M_new": "mixture8M_s101", "lattice2M": "lattice128",
+               "sphere1M": "unit_sphere1M", "uniform100k": "uniform100k"}
 
 
-def _canon_digest(tets):
-    from wtet_b200.autotune import tet_set_digest
+def golden_digests():
+    p = os.path.join(ROOT, "tests", "golden", "full_size.json")
+    if not os.path.exists(p):
+        return {}
+    with open(p) as f:
+        return json.load(f)
 
-    return tet_set_digest(tets)
+
+def device_digest(wt, d_t, d_a, m, n):
+    """Canonical form of the first m output rows on the device, as SHA-256."""
+    ct, ca = wt.canonical_device(d_t[:m], d_a[:m], n)
+    return wt.canonical_digest(ct, ca)
 
 
-def variants(wt, args):
+def device_run(wt, L, d_pts, n, cfg, d_t, d_a, cap, stream):
+    m = ctypes.c_uint64(0)
+    st = wt._core.Stats()
+    rc = L.wtet_delaunay_device(ctypes.c_void_p(d_pts.data_ptr()), n, ctypes.byref(cfg),
+                                ctypes.c_void_p(d_t.data_ptr()), ctypes.c_void_p(d_a.data_ptr()), cap,
+                                ctypes.byref(m), ctypes.byref(st), ctypes.c_void_p(stream.cuda_stream))
+    if rc != 0:
+        raise RuntimeError(L.wtet_last_error().decode())
+    return m.value, st
+
+
+def variants(wt, args, golden):
     """The metric's other two forms, each on its own configuration, device
-    time (CUDA events inside the library), with the tet sets compared:
-    learned vs plain scheduler on 8M mixture points from an unseen seed, and
-    4,096 batched clouds in one call vs looping the plain path over them."""
+    time (CUDA events inside the library), each output compared with the
+    oracle's stored canonical digest:
+      learned  8M mixture clouds from seeds 101-105 (no training run saw them),
+               plain vs learned scheduler;
+      learned_lattice  the 128^3 lattice, plain vs learned;
+      batched  4,096 clouds in one call vs looping the plain path over them."""
+    import torch
+
+    from wtet_b200 import synthetic as syn
+
+    L = wt._core.load()
+    stream = torch.cuda.current_stream()
+    reps = 3
     out = {}
-    reps = max(2, min(args.steps, 3))
-    pts = make_workload("mixture8M_new")[0]
-    res = {}
-    for vote in ("plain", "learned"):
-        cfg = wt.Config(vote=vote)
-        wt.delaunay(pts, cfg)
-        runs = [wt.delaunay(pts, cfg) for _ in range(reps)]
-        ms = float(np.median([r.stats["device_ms"] for r in runs]))
-        res[vote] = (runs[-1], ms)
-    same = _canon_digest(res["plain"][0].tets) == _canon_digest(res["learned"][0].tets)
+
+    def measure(pts, vote, gname):
+        n = len(pts)
+        d_pts = torch.from_numpy(pts).cuda()
+        cap = int(L.wtet_max_tets(n))
+        d_t = torch.empty((cap, 4), dtype=torch.int32, device="cuda")
+        d_a = torch.empty((cap, 4), dtype=torch.int32, device="cuda")
+        cfg = wt.Config(vote=vote)._c()
+        device_run(wt, L, d_pts, n, cfg, d_t, d_a, cap, stream)
+        runs = [device_run(wt, L, d_pts, n, cfg, d_t, d_a, cap, stream) for _ in range(reps)]
+        m, st = runs[-1]
+        dig = device_digest(wt, d_t, d_a, m, n)
+        ms = float(np.median([r[1].device_ms for r in runs]))
+        rec = {"mpts": round(n / (ms * 1e3), 3), "device_ms": round(ms, 2), "rounds": int(st.rounds),
+               "vote_winners": int(st.vote_winners), "cavity_searches": int(st.candidates),
+               "same_as_oracle": bool(gname in golden and dig == golden[gname]["sha256"])}
+        del d_t, d_a, d_pts
+        torch.cuda.empty_cache()
+        return rec
+
+    seeds = []
+    for seed in range(101, 106):
+        pts = syn.mixture(8_000_000, seed)
+        rec = {"seed": seed}
+        for vote in ("plain", "learned"):
+            for k, v in measure(pts, vote, f"mixture8M_s{seed}").items():
+                rec[f"{vote}_{k}"] = v
+        seeds.append(rec)
     out["learned"] = {
-        "workload": "mixture8M_new", "same_tet_set": same,
-        **{f"{v}_{k}": val for v in ("plain", "learned") for k, val in (
-            ("mpts", round(len(pts) / (res[v][1] * 1e3), 3)),
-            ("device_ms", round(res[v][1], 2)),
-            ("rounds", int(res[v][0].stats["rounds"])),
-            ("vote_winners", int(res[v][0].stats["vote_winners"])),
-            ("cavity_searches", int(res[v][0].stats["candidates"])))},
+        "workload": "8,000,000-point mixture clouds, seeds 101-105",
+        "per_seed": seeds,
+        "plain_mpts_mean": round(float(np.mean([r["plain_mpts"] for r in seeds])), 3),
+        "learned_mpts_mean": round(float(np.mean([r["learned_mpts"] for r in seeds])), 3),
+        "learned_faster_on": sum(r["learned_mpts"] > r["plain_mpts"] for r in seeds),
+        "all_same_as_oracle": all(r["plain_same_as_oracle"] and r["learned_same_as_oracle"] for r in seeds),
     }
-    # the degenerate configuration, where large cavities make searches expensive
-    lat = make_workload("lattice2M")[0]
-    resl = {}
-    for vote in ("plain", "learned"):
-        cfg = wt.Config(vote=vote)
-        wt.delaunay(lat, cfg)
-        runs = [wt.delaunay(lat, cfg) for _ in range(2)]
-        resl[vote] = (runs[-1], float(np.median([r.stats["device_ms"] for r in runs])))
-    out["learned_lattice"] = {
-        "workload": "lattice2M",
-        "same_tet_set": _canon_digest(resl["plain"][0].tets) == _canon_digest(resl["learned"][0].tets),
-        **{f"{v}_{k}": val for v in ("plain", "learned") for k, val in (
-            ("mpts", round(len(lat) / (resl[v][1] * 1e3), 3)),
-            ("device_ms", round(resl[v][1], 1)),
-            ("rounds", int(resl[v][0].stats["rounds"])),
-            ("cavity_searches", int(resl[v][0].stats["candidates"])))},
-    }
+    lat = syn.lattice(128)
+    out["learned_lattice"] = {"workload": "lattice2M",
+                              **{f"{v}_{k}": x for v in ("plain", "learned")
+                                 for k, x in measure(lat, v, "lattice128").items()}}
     clouds = make_workload("batched")
     n = sum(len(c) for c in clouds)
     wt.delaunay_batched(clouds)
@@ -430,30 +509,42 @@ def variants(wt, args):
     for _ in range(reps):
         rb = wt.delaunay_batched(clouds)
         bms.append(rb[0].stats["device_ms"])
-    loop_ms = 0.0
     same_b = True
-    for c, r in zip(clouds, rb):
-        ra = wt.delaunay(c)
-        loop_ms += ra.stats["device_ms"]
-        same_b = same_b and _canon_digest(ra.tets) == _canon_digest(r.tets)
+    gb = os.path.join(ROOT, "tests", "golden", "batched_digests.npz")
+    if os.path.exists(gb):
+        want = np.load(gb)["digests"]
+        for i, (c, r) in enumerate(zip(clouds, rb)):
+            ct, ca = wt.canonical(r.tets, r.adjacency, len(c))
+            same_b = same_b and bytes.fromhex(wt.canonical_digest(ct, ca)) == want[i].tobytes()
+    else:
+        same_b = None
+    loop_ms = 0.0
+    for c in clouds:
+        loop_ms += wt.delaunay(c).stats["device_ms"]
     bm = float(np.median(bms))
-    out["batched"] = {"workload": "batched", "clouds": len(clouds), "points": n, "same_tet_sets": same_b,
+    out["batched"] = {"workload": "batched", "clouds": len(clouds), "points": n, "all_same_as_oracle": same_b,
                       "batched_mpts": round(n / (bm * 1e3), 3), "batched_device_ms": round(bm, 1),
-                      "looped_plain_mpts": round(n / (loop_ms * 1e3), 3), "looped_device_ms": round(loop_ms, 1)}
+                      "looped_plain_mpts": round(n / (loop_ms * 1e3), 3), "looped_device_ms": round(loop_ms, 1),
+                      "how": "one job over all clouds, insertion rounds replayed from CUDA graphs (no persistent "
+                             "kernel: consecutive graph nodes are the grid-wide barriers)"}
     return out
 
 
-def cpu_baseline(points, sample: int):
-    """The oracle (sequential exact Bowyer-Watson) on the first `sample` points."""
+def cpu_baseline(points, gpu_digest):
+    """The oracle (the reference's exact Bowyer-Watson, src/phase2.rs:383-606,
+    restated with walk point location) on the whole workload, one core; its
+    canonical output is compared with the GPU's."""
     import oracle
 
-    sub = np.ascontiguousarray(points[:sample])
+    oracle.build()
+    pts = np.ascontiguousarray(points)
     t0 = time.perf_counter()
-    oracle.delaunay(sub, 1)
+    tets, adj, _ = oracle.delaunay(pts, 1)
     dt = time.perf_counter() - t0
-    return {"value": round(len(sub) / dt / 1e6, 4), "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"first {len(sub)} points of the same workload, one oracle triangulation ({dt:.1f} s)",
-            "host_cpu": host_cpu()}
+    od = oracle.digest(*oracle.canonical(tets, adj, len(pts)))
+    return {"value": round(len(pts) / dt / 1e6, 4), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"the whole workload ({len(pts)} points), one oracle triangulation on one core ({dt:.1f} s)",
+            "host_cpu": host_cpu(), "oracle_digest": od, "gpu_output_identical": od == gpu_digest}
 
 
 def host_cpu():
@@ -468,8 +559,11 @@ def host_cpu():
 
 
 def run_reference(args):
-    """CPU reference arm: the oracle port on all host cores (independent
-    samples of the workload triangulated concurrently)."""
+    """CPU reference arm: the reference's CPU algorithm (the oracle port of
+    src/phase2.rs:383-606 with walk point location; the Rust/wgpu reference
+    cannot be built or run here) on every host core.  A step is one complete
+    triangulation of the same workload as the GPU arm; the threads take steps
+    from a queue (W untimed warm-up steps first, then exactly K timed steps)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -480,34 +574,34 @@ def run_reference(args):
     oracle.build()
     clouds = make_workload(args.workload)
     threads = max(1, os.cpu_count() or 1)
-    if len(clouds) == 1:
-        pts = clouds[0]
-        chunk = min(args.cpu_sample, len(pts) // threads) if threads > 1 else args.cpu_sample
-        samples = [np.ascontiguousarray(pts[i * chunk:(i + 1) * chunk]) for i in range(threads)]
-    else:
-        samples = clouds[: threads * 4]
-    npts = sum(len(s) for s in samples)
 
     def one_step():
-        with cf.ThreadPoolExecutor(threads) as ex:
-            list(ex.map(lambda p: oracle.delaunay(p, 1), samples))
+        for c in clouds:
+            oracle.triangulate_count(c, 1)
 
-    for _ in range(args.warmup if args.warmup < 2 else 1):
-        one_step()
+    def run_steps(k):
+        if k <= 0:
+            return
+        with cf.ThreadPoolExecutor(min(threads, k)) as ex:
+            list(ex.map(lambda _: one_step(), range(k)))
+
+    run_steps(args.warmup)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        one_step()
+    run_steps(args.steps)
     ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    npts = sum(len(c) for c in clouds)
     v = npts / (ms * 1e3)
-    desc = f"{len(samples)} independent samples of {npts // len(samples)} points on {threads} threads"
+    desc = (f"{args.steps} complete triangulations of the workload ({npts} points each), "
+            f"up to {min(threads, args.steps)} at a time on {threads} threads")
     out = {"impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": args.workload, "description": WORKLOADS[args.workload]},
+           "config": bench_config(args.workload, args.vote, 1),
            "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": threads, "kind": "port", "sample": desc,
                             "host_cpu": host_cpu()},
            "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-           "note": "reference CPU algorithm restated (oracle/); the Rust+wgpu reference cannot be built or run here"}
+           "note": "the reference's CPU algorithm restated (oracle/); its Rust + wgpu path cannot be built "
+                   "or run on this machine"}
     print(json.dumps(out), flush=True)
 
 
@@ -519,7 +613,6 @@ def main():
     ap.add_argument("--impl", default="wtet_b200", choices=["wtet_b200", "reference"])
     ap.add_argument("--workload", default="mixture8M", choices=sorted(WORKLOADS))
     ap.add_argument("--vote", default="plain", choices=["plain", "learned"])
-    ap.add_argument("--cpu-sample", type=int, default=2_000_000)
     ap.add_argument("--no-variants", dest="variants", action="store_false",
                     help="skip the learned-scheduler and batched measurements")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -229,6 +229,21 @@ def delaunay(points, order_mode: int = 1):
     return tets, adj, d
 
 
+def triangulate_count(points, order_mode: int = 1) -> int:
+    """Runs the oracle triangulation and returns its tet count without
+    copying the output out (for timing the CPU path: the run itself still
+    builds the compacted output rows, as the reference's readback does)."""
+    pts = _f32(points)
+    st = OracleStats()
+    h = lib().oracle_dt_run(_ptr(pts), pts.shape[0], order_mode, ctypes.byref(st))
+    if not h:
+        raise RuntimeError("oracle: " + lib().oracle_last_error().decode())
+    try:
+        return int(lib().oracle_dt_num_tets(h))
+    finally:
+        lib().oracle_dt_free(h)
+
+
 def check_delaunay_quality(points, tets, adj) -> int:
     pts = _f32(points)
     t = np.ascontiguousarray(tets, np.uint32)

@@ -27,7 +27,8 @@ constexpr double kIspBoundA = (16.0 + 224.0 * kEps) * kEps;
 // src/predicates.rs:426-427
 constexpr double kO3dBoundLifted = (11.0 + 112.0 * kEps) * kEps;
 
-PredStats g_stats{};
+// per thread: concurrent triangulations (the CPU reference arm) share nothing
+thread_local PredStats g_stats{};
 
 // 2-component expansion of a*b (increasing magnitude).
 inline int prod2(double a, double b, double* h) {

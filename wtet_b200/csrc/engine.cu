@@ -12,9 +12,8 @@
 // equivalent to some sequential order.  The result is therefore the unique
 // SoS Delaunay triangulation, with no flip failures and nothing left to repair.
 //
-// Round structure (one insertion round over all clouds of a job; 13 kernels
-// replayed from a CUDA graph, 15 with the learned scheduler):
-//   k_begin       start the next stratum when the current one has thinned
+// Round structure (one insertion round over all clouds of a job; 10 kernels
+// replayed from a CUDA graph, 12 with the learned scheduler):
 //   k_activate    locate the new stratum's points (walk from the curve
 //                 predecessor's tet)
 //   k_vote        each uninserted point votes for its tet (64-bit atomicMax of
@@ -33,15 +32,19 @@
 //   k_shared      two winners whose cavities share a face both stay only if
 //                 that face remains Delaunay (exact insphere); else the worse
 //                 one steps back -- this exact test replaces a blanket
-//                 exclusion of neighbouring cavities
-//   k_alloc       recycled / fresh slots for the new tets
+//                 exclusion of neighbouring cavities; the winners that stay
+//                 get recycled / fresh slots for their new tets
 //   k_write       new tets written, adjacency stitched through an edge table
 //                 (rotation around boundary edges for the very largest
 //                 cavities), cavity retired
 //   k_relocate    points whose tet was retired walk (exact orient3d) from a
 //                 tet of the inserting point; the rest keep their tet; the
-//                 uninserted list is compacted with warp-aggregated appends
-//   k_carry, k_end  recycled-slot carry-over, list swap, stop conditions
+//                 uninserted list is compacted with warp-aggregated appends;
+//                 unused recycled slots carry over
+//   k_end         list swap, stop conditions, and the next round's start:
+//                 the next stratum once the current one has thinned
+// The cavity search, shared-face test and tet writing take their work items
+// dynamically (atomic cursors): cavity sizes vary by orders of magnitude.
 // Strata: points are bucketed per cloud along a Morton (or Hilbert) curve
 // (counting sort) and inserted in the reference's stratified stride order
 // (src/gpu/mod.rs:533-600), each new stratum located by a walk from its
@@ -102,6 +105,7 @@ struct Counters {
   uint32_t n_inserted;    // winners this round
   uint32_t huge_used;     // huge-cavity slots used
   uint32_t btab_used;     // k_write's large edge tables handed out this round
+  uint32_t work[4];       // dynamic work cursors of k_bfs, k_shared, k_write, k_resolve
   uint32_t err;           // error flags
   unsigned long long walk_steps;
   unsigned long long n_expanded;
@@ -131,6 +135,9 @@ struct alignas(16) State {
   uint32_t log_used;      // scheduler training records reserved
   unsigned long long inserted;
   unsigned long long starts;  // vote winners that attempted an insertion
+  // the last finished round's counts (the counters are reset when the next
+  // round starts)
+  uint32_t last_starts, last_cand, last_inserted, last_alloc;
 };
 
 // Everything a kernel needs, passed by value.
@@ -165,7 +172,7 @@ struct Dev {
   uint32_t* cand_off;  // pool offset, or BIG flag | big slot
   uint32_t* cand_len;
   uint32_t* cand_base;
-  uint32_t* cand_nf;   // boundary faces of each winning candidate (k_alloc)
+  uint32_t* cand_nf;   // boundary faces of each winning candidate (k_shared)
   uint8_t* st1;  // candidate owns its whole cavity
   uint8_t* st2;  // ... and no shared face with a better winner is violated
   uint32_t* bigcand;  // points taking the huge-cavity path this round
@@ -189,6 +196,8 @@ struct Dev {
   uint8_t* losses;          // vote wins of each point that did not insert
   const mlp::Image* mlp;    // inference weights
   uint8_t* ring2;           // learned scheduler: the winner pre-claims two rings of neighbours
+  uint8_t* prio;            // learned scheduler: claim priority class of each winner (smaller first)
+  uint32_t sched_mode;      // learned scheduler: bit 0 ring radius from the score, bit 1 priority class
   float deep_threshold;     // learned scheduler: predicted probability above which it does
   float* log_x;             // logged features (log_cap x 12)
   uint8_t* log_y;           // logged labels: the winner inserted this round
@@ -268,14 +277,17 @@ __device__ __forceinline__ uint32_t mix32(uint32_t h) {
 // they would wait until their whole neighbourhood is quiet.  Every other
 // candidate has priority 1.
 __device__ __forceinline__ unsigned long long make_key(const Dev& D, const RoundArgs& R, uint32_t p) {
-  const unsigned long long prio = D.bigflag[p] == 2 ? 0u : 1u;
+  const unsigned long long prio = D.bigflag[p] == 2 ? 0u : 1u + (D.prio ? D.prio[p] : 0u);
   return R.stamp | (prio << 32) | mix32(p ^ (R.round * 0x9E3779B9u));
 }
 
-// Grid-stride loop in which each warp takes one item (warp-uniform).
-#define WARP_LOOP(ci, count)                                                              \
-  for (uint32_t ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ci < (count);         \
-       ci += (gridDim.x * blockDim.x) >> 5)
+// Next work item of a warp-per-item kernel (dynamic: items differ widely in
+// cost, so warps that finish early take more).
+__device__ __forceinline__ uint32_t warp_next(uint32_t* cursor) {
+  uint32_t v = 0;
+  if ((threadIdx.x & 31) == 0) v = atomicAdd(cursor, 1u);
+  return __shfl_sync(0xFFFFFFFFu, v, 0);
+}
 
 // Appends `pred` lanes to a list through one atomic per warp.
 __device__ __forceinline__ uint32_t warp_append(uint32_t* ctr, bool pred) {
@@ -762,8 +774,10 @@ __global__ void __launch_bounds__(128) k_sched(Dev D) {
     if (valid) {
       float sc = outs[w][lane];
       sc = (sc == sc) ? fminf(fmaxf(sc, -20.f), 20.f) : -20.f;
-      const bool two = 1.f / (1.f + __expf(-sc)) > D.deep_threshold;
+      const float prob = 1.f / (1.f + __expf(-sc));
+      const bool two = (D.sched_mode & 1u) && prob > D.deep_threshold;
       D.ring2[p] = two ? 1 : 0;
+      if (D.prio) D.prio[p] = (D.sched_mode & 2u) ? uint8_t(min(3, int(prob * 4.f))) : 0;
       if (D.prefilter) pre_claim(D, t, make_key(D, R, p), two);
     }
     __syncwarp();
@@ -853,26 +867,50 @@ __global__ void k_cands(Dev D) {
 // huge path next round.
 constexpr uint32_t kBfsLanes = 16;
 constexpr uint32_t kWarpGroups = 32 / kBfsLanes;
-constexpr uint32_t kBfsShared = 128;  // queue entries per group in shared memory
+constexpr uint32_t kBfsShared = 64;  // queue entries (tet + neighbour words) per group in shared memory
 // Learned scheduler label: a cavity of more tets than a two-ring pre-claim
 // (17) covers is "large".
 constexpr uint32_t kLargeCavity = 17;
+
+// Loads issued as written (volatile asm is neither sunk into the branch that
+// uses the value nor merged with later loads), so that a pass of the cavity
+// search issues its claim, memo, vertex and neighbour loads together.
+__device__ __forceinline__ uint4 ld_nc_u4(const uint4* p) {
+  uint4 v;
+  asm volatile("ld.global.nc.v4.u32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(p));
+  return v;
+}
+__device__ __forceinline__ unsigned long long ld_cg_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.global.cg.u64 %0, [%1];" : "=l"(v) : "l"(p));
+  return v;
+}
 
 __global__ void __launch_bounds__(128, 8) k_bfs(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
   constexpr uint32_t FULL = 0xFFFFFFFFu, GM = (kBfsLanes == 32) ? 0xFFFFFFFFu : ((1u << kBfsLanes) - 1u);
+  // queue of each lane group: cavity tets and their four neighbour words
   __shared__ uint32_t sq_all[4 * kWarpGroups][kBfsShared];
+  __shared__ uint4 sn_all[4 * kWarpGroups][kBfsShared];
   const uint32_t lane = threadIdx.x & 31, gl = lane % kBfsLanes, shift = lane - gl;
   const uint32_t lt = (1u << gl) - 1u;
   const uint32_t gid = (blockIdx.x * blockDim.x + threadIdx.x) / kBfsLanes;  // global group index
-  const uint32_t ngroups = gridDim.x * blockDim.x / kBfsLanes;
   uint32_t* sq = sq_all[threadIdx.x / kBfsLanes];
+  uint4* sn = sn_all[threadIdx.x / kBfsLanes];
   uint32_t* cav = D.wscratch + size_t(gid) * BIG_CAP;
   const uint32_t nstart = __ldcg(&D.ctr->big_used);
-  const uint32_t first = gid - gid % kWarpGroups;  // the warp's first group: warp-uniform loop bounds
-  for (uint32_t base = first; base < nstart; base += ngroups) {
-    const uint32_t si = base + gid % kWarpGroups;
+  // Work is taken dynamically, kWarpGroups consecutive starts per warp:
+  // cavities differ in size by orders of magnitude, and a static grid-stride
+  // split leaves warps idle behind the slowest ones.
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&D.ctr->work[0], kWarpGroups);
+    base = __shfl_sync(FULL, base, 0);
+    if (base >= nstart) break;  // warp-uniform
+    const uint32_t si = base + lane / kBfsLanes;
     bool active = si < nstart;
     uint32_t p = 0, t0 = 0;
     if (active) {
@@ -901,6 +939,7 @@ __global__ void __launch_bounds__(128, 8) k_bfs(Dev D) {
       const unsigned long long old = atomicMin(&D.ccav[t0], key);
       claim_lost = old < key;
       sq[0] = t0;
+      sn[0] = D.tn[t0];
     }
     const int g_claim = __shfl_sync(FULL, claim_lost, shift);
     bool lost = !searched || g_claim;
@@ -911,32 +950,41 @@ __global__ void __launch_bounds__(128, 8) k_bfs(Dev D) {
     while (__any_sync(FULL, running)) {
       bool add = false, my_lost = false, my_guard = false;
       uint32_t nt = 0;
+      uint4 nn = make_uint4(NONE, NONE, NONE, NONE);
       const uint32_t idx = head + gl / 4u;
       const uint32_t f = gl & 3u;
       if (running && idx < K) {
-        const uint32_t c = idx < kBfsShared ? sq[idx] : cav[idx];
-        const uint32_t nb = reinterpret_cast<const uint32_t*>(D.tn + c)[f];
+        // the neighbour word comes from the queue (loaded when the tet was
+        // added), or from global memory for entries beyond the shared part
+        const uint32_t nb = idx < kBfsShared ? comp(sn[idx], int(f))
+                                             : reinterpret_cast<const uint32_t*>(D.tn + cav[idx])[f];
         if (nb != NONE) {
           nt = nb >> 2;
           if (nt >= D.cap) {
             my_guard = true;
-          } else if (__ldcg(&D.ccav[nt]) != key && __ldcg(&D.cring[nt]) != key) {
-            const uint4 W = D.tv[nt];
-            if (W.x >= D.nv || W.y >= D.nv || W.z >= D.nv || W.w >= D.nv) {
-              my_guard = true;
-            } else {
-              double P[4][3];
-              load_pt(D.pts, W.x, P[0]);
-              load_pt(D.pts, W.y, P[1]);
-              load_pt(D.pts, W.z, P[2]);
-              load_pt(D.pts, W.w, P[3]);
-              const int sg = o4d_sos(P[0], P[1], P[2], P[3], pp, W.x, W.y, W.z, W.w, p, D.sos, &D.ctr->err);
-              if (sg < 0) {
-                const unsigned long long old = atomicMin(&D.ccav[nt], key);
-                if (old < key) my_lost = true;
-                else if (old != key) add = true;
+          } else {
+            // one round trip: claim, memo, vertices and neighbours together
+            const unsigned long long cc = ld_cg_u64(&D.ccav[nt]);
+            const unsigned long long cr = ld_cg_u64(&D.cring[nt]);
+            const uint4 W = ld_nc_u4(D.tv + nt);
+            nn = ld_nc_u4(D.tn + nt);
+            if (cc != key && cr != key) {
+              if (W.x >= D.nv || W.y >= D.nv || W.z >= D.nv || W.w >= D.nv) {
+                my_guard = true;
               } else {
-                D.cring[nt] = key;  // memo for this candidate only
+                double P[4][3];
+                load_pt(D.pts, W.x, P[0]);
+                load_pt(D.pts, W.y, P[1]);
+                load_pt(D.pts, W.z, P[2]);
+                load_pt(D.pts, W.w, P[3]);
+                const int sg = o4d_sos(P[0], P[1], P[2], P[3], pp, W.x, W.y, W.z, W.w, p, D.sos, &D.ctr->err);
+                if (sg < 0) {
+                  const unsigned long long old = atomicMin(&D.ccav[nt], key);
+                  if (old < key) my_lost = true;
+                  else if (old != key) add = true;
+                } else {
+                  D.cring[nt] = key;  // memo for this candidate only
+                }
               }
             }
           }
@@ -946,9 +994,14 @@ __global__ void __launch_bounds__(128, 8) k_bfs(Dev D) {
       const uint32_t pos = K + __popc(gball & lt);
       bool my_over = false;
       if (add) {
-        if (pos < kBfsShared) sq[pos] = nt;
-        else if (pos < BIG_CAP) cav[pos] = nt;
-        else my_over = true;
+        if (pos < kBfsShared) {
+          sq[pos] = nt;
+          sn[pos] = nn;
+        } else if (pos < BIG_CAP) {
+          cav[pos] = nt;
+        } else {
+          my_over = true;
+        }
       }
       const bool g_guard = (__ballot_sync(FULL, my_guard) >> shift) & GM;
       const bool g_lost = (__ballot_sync(FULL, my_lost) >> shift) & GM;
@@ -1100,7 +1153,7 @@ __global__ void k_resolve(Dev D) {
   if (!R.live) return;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t ncand = __ldcg(&D.ctr->n_cand);
-  WARP_LOOP(ci, ncand) {
+  for (uint32_t ci = warp_next(&D.ctr->work[3]); ci < ncand; ci = warp_next(&D.ctr->work[3])) {
     uint32_t p = D.cand[ci];
     uint32_t K = D.cand_len[ci];
     const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
@@ -1113,57 +1166,12 @@ __global__ void k_resolve(Dev D) {
   }
 }
 
-// Two winners whose cavities share a face f may both insert iff f stays
-// Delaunay: the better winner q must lie outside the circumsphere of the
-// worse winner p's new tet on f (then either insertion order gives the same
-// tets).  The worse one of a violating pair steps back.
-__global__ void __launch_bounds__(128, 8) k_shared(Dev D) {
-  const RoundArgs R = load_round(D);
-  if (!R.live) return;
-  const uint32_t lane = threadIdx.x & 31;
-  const uint32_t ncand = __ldcg(&D.ctr->n_cand);
-  WARP_LOOP(ci, ncand) {
-    uint32_t p = D.cand[ci];
-    if (!D.st1[p]) {
-      if (lane == 0) D.st2[p] = 0;
-      continue;
-    }
-    uint32_t K = D.cand_len[ci];
-    const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
-    unsigned long long key = make_key(D, R, p);
-    bool bad = false;
-    double pp[3];
-    load_pt(D.pts, p, pp);
-    // one lane per (cavity tet, face)
-    for (uint32_t e = lane; e < 4 * K && !bad; e += 32) {
-      const uint32_t c = cav[e >> 2];
-      const int f = int(e & 3u);
-      {
-        uint32_t nb = reinterpret_cast<const uint32_t*>(D.tn + c)[f];
-        if (nb == NONE) continue;
-        unsigned long long cc = __ldcg(&D.ccav[nb >> 2]);
-        if (cc >= key || !this_round(R, cc)) continue;
-        uint32_t q = key_owner(R, cc);
-        if (q >= D.nv || !D.st1[q]) continue;
-        const uint4 V = D.tv[c];
-        uint32_t w[4];
-        double P[4][3];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {  // the new tet on face f: p replaces vertex f
-          w[k] = k == f ? p : comp(V, k);
-          load_pt(D.pts, w[k], P[k]);
-        }
-        double qq[3];
-        load_pt(D.pts, q, qq);
-        if (o4d_sos(P[0], P[1], P[2], P[3], qq, w[0], w[1], w[2], w[3], q, D.sos, &D.ctr->err) < 0) {
-          bad = true;
-          break;
-        }
-      }
-    }
-    bool viol = __any_sync(0xFFFFFFFFu, bad);
-    if (lane == 0) D.st2[p] = viol ? 0 : 1;
-  }
+__device__ __forceinline__ uint32_t slot_of(const Dev& D, const RoundArgs& R, uint32_t v) {
+  return v < R.n_freed_prev ? R.freed_prev[v] : R.tet_top + (v - R.n_freed_prev);
+}
+
+__device__ __forceinline__ bool boundary_face(const Dev& D, uint32_t nb, unsigned long long key) {
+  return nb == NONE || __ldcg(&D.ccav[nb >> 2]) != key;
 }
 
 // The edge of face f of tet V opposite corner k (k != f): its two vertex ids,
@@ -1179,41 +1187,72 @@ __device__ __forceinline__ uint32_t edge_hi(const uint4& V, int f, int k) {
   return max(comp(V, q0), comp(V, q1));
 }
 
-__device__ __forceinline__ uint32_t slot_of(const Dev& D, const RoundArgs& R, uint32_t v) {
-  return v < R.n_freed_prev ? R.freed_prev[v] : R.tet_top + (v - R.n_freed_prev);
-}
-
-__device__ __forceinline__ bool boundary_face(const Dev& D, uint32_t nb, unsigned long long key) {
-  return nb == NONE || __ldcg(&D.ccav[nb >> 2]) != key;
-}
-
-// Hands out one slot per boundary face (recycled slots first, then fresh ones).
-__global__ void k_alloc(Dev D) {
+// Two winners whose cavities share a face f may both insert iff f stays
+// Delaunay: the better winner q must lie outside the circumsphere of the
+// worse winner p's new tet on f (then either insertion order gives the same
+// tets).  The worse one of a violating pair steps back.  A winner that stays
+// is handed one slot per boundary face (recycled slots first, then fresh
+// ones) in the same pass over its cavity.
+__global__ void __launch_bounds__(128, 8) k_shared(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
+  constexpr uint32_t FULL = 0xFFFFFFFFu;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t ncand = __ldcg(&D.ctr->n_cand);
-  WARP_LOOP(ci, ncand) {
-    uint32_t p = D.cand[ci];
-    if (!D.st2[p]) continue;
-    uint32_t K = D.cand_len[ci];
+  for (uint32_t ci = warp_next(&D.ctr->work[1]); ci < ncand; ci = warp_next(&D.ctr->work[1])) {
+    const uint32_t p = D.cand[ci];
+    if (!D.st1[p]) {
+      if (lane == 0) D.st2[p] = 0;
+      continue;
+    }
+    const uint32_t K = D.cand_len[ci];
     const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
-    unsigned long long key = make_key(D, R, p);
-    uint32_t Fl = 0;
-    for (uint32_t i = lane; i < K; i += 32) {
-      uint4 N = D.tn[cav[i]];
-      for (int f = 0; f < 4; ++f) Fl += boundary_face(D, comp(N, f), key);
+    const unsigned long long key = make_key(D, R, p);
+    double pp[3];
+    load_pt(D.pts, p, pp);
+    // one lane per (cavity tet, face): boundary faces are counted (their
+    // flags kept in a register for cavities of up to 64 tets), faces shared
+    // with a better winner are tested
+    bool bad = false;
+    uint32_t total = 0, bmask = 0;
+    for (uint32_t e0 = 0; e0 < 4 * K; e0 += 32) {
+      const uint32_t e = e0 + lane;
+      bool bnd = false;
+      if (e < 4 * K) {
+        const uint32_t c = cav[e >> 2];
+        const int f = int(e & 3u);
+        const uint32_t nb = reinterpret_cast<const uint32_t*>(D.tn + c)[f];
+        const unsigned long long cc = nb == NONE ? 0ull : __ldcg(&D.ccav[nb >> 2]);
+        bnd = nb == NONE || cc != key;
+        if (bnd && nb != NONE && !bad && cc < key && this_round(R, cc)) {
+          const uint32_t q = key_owner(R, cc);
+          if (q < D.nv && D.st1[q]) {
+            const uint4 V = D.tv[c];
+            uint32_t w[4];
+            double P[4][3];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {  // the new tet on face f: p replaces vertex f
+              w[k] = k == f ? p : comp(V, k);
+              load_pt(D.pts, w[k], P[k]);
+            }
+            double qq[3];
+            load_pt(D.pts, q, qq);
+            if (o4d_sos(P[0], P[1], P[2], P[3], qq, w[0], w[1], w[2], w[3], q, D.sos, &D.ctr->err) < 0) bad = true;
+          }
+        }
+      }
+      const uint32_t ball = __ballot_sync(FULL, bnd);
+      total += __popc(ball);
+      if (e0 < 256 && bnd) bmask |= 1u << (e0 >> 5);
     }
-    uint32_t incl = Fl;
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-      if (lane >= uint32_t(o)) incl += y;
+    if (__any_sync(FULL, bad)) {
+      if (lane == 0) D.st2[p] = 0;
+      continue;
     }
-    uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
     uint32_t base = 0;
     if (lane == 0) base = atomicAdd(&D.ctr->alloc_used, total);
-    base = __shfl_sync(0xFFFFFFFFu, base, 0);
-    uint32_t last = base + total;
+    base = __shfl_sync(FULL, base, 0);
+    const uint32_t last = base + total;
     if (last > R.n_freed_prev && R.tet_top + (last - R.n_freed_prev) > D.cap) {
       if (lane == 0) {
         atomicOr(&D.ctr->err, kErrCapacity);
@@ -1221,18 +1260,33 @@ __global__ void k_alloc(Dev D) {
       }
       continue;
     }
-    uint32_t j = base + incl - Fl;
-    for (uint32_t i = lane; i < K; i += 32) {
-      uint32_t c = cav[i];
-      uint4 N = D.tn[c];
-      uint4 S = make_uint4(NONE, NONE, NONE, NONE);
-      for (int f = 0; f < 4; ++f)
-        if (boundary_face(D, comp(N, f), key)) set_comp(S, f, slot_of(D, R, j++));
-      D.nslot[c] = S;
+    // slots in (tet, face) order; inner faces get NONE
+    uint32_t run = 0;
+    for (uint32_t e0 = 0; e0 < 4 * K; e0 += 32) {
+      const uint32_t e = e0 + lane;
+      bool bnd = false;
+      uint32_t c = 0;
+      int f = 0;
+      if (e < 4 * K) {
+        c = cav[e >> 2];
+        f = int(e & 3u);
+        if (4 * K <= 256) {
+          bnd = (bmask >> (e0 >> 5)) & 1u;
+        } else {
+          const uint32_t nb = reinterpret_cast<const uint32_t*>(D.tn + c)[f];
+          bnd = boundary_face(D, nb, key);
+        }
+      }
+      const uint32_t ball = __ballot_sync(FULL, bnd);
+      if (e < 4 * K)
+        reinterpret_cast<uint32_t*>(D.nslot + c)[f] =
+            bnd ? slot_of(D, R, base + run + __popc(ball & ((1u << lane) - 1u))) : NONE;
+      run += __popc(ball);
     }
     if (lane == 0) {
       D.cand_base[ci] = base;
       D.cand_nf[ci] = total;
+      D.st2[p] = 1;
     }
   }
 }
@@ -1267,13 +1321,13 @@ __global__ void __launch_bounds__(128, 8) k_write(Dev D) {
   const uint32_t w = threadIdx.x >> 5;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t ncand = __ldcg(&D.ctr->n_cand);
-  WARP_LOOP(ci, ncand) {
+  for (uint32_t ci = warp_next(&D.ctr->work[2]); ci < ncand; ci = warp_next(&D.ctr->work[2])) {
     uint32_t p = D.cand[ci];
     if (!D.st2[p]) continue;
     uint32_t K = D.cand_len[ci];
     const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
     unsigned long long key = make_key(D, R, p);
-    const uint32_t F = D.cand_nf[ci];  // boundary faces, counted by k_alloc
+    const uint32_t F = D.cand_nf[ci];  // boundary faces, counted by k_shared
     unsigned long long* tk = nullptr;
     uint32_t *t0 = nullptr, *t1 = nullptr;
     uint32_t mask = 31;
@@ -1440,8 +1494,9 @@ __global__ void __launch_bounds__(128, 8) k_write(Dev D) {
   }
 }
 
-// Clears the votes, relocates points whose tet was retired, and compacts the
-// uninserted list.
+// Clears the votes, relocates points whose tet was retired, compacts the
+// uninserted list, and carries the recycled slots that were not handed out
+// this round over to the next round's list.
 __global__ void __launch_bounds__(512, 2) k_relocate(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
@@ -1478,12 +1533,21 @@ __global__ void __launch_bounds__(512, 2) k_relocate(Dev D) {
     if (keep) R.active_next[slot] = p;
   }
   if (steps) atomicAdd(&D.ctr->walk_steps, (unsigned long long)steps);
+  // recycled slots not handed out this round (k_write has appended this
+  // round's retired tets in front of them)
+  const uint32_t used = __ldcg(&D.ctr->alloc_used);
+  if (R.n_freed_prev > used) {
+    const uint32_t nfn = __ldcg(&D.ctr->n_freed_next);
+    const uint32_t left = R.n_freed_prev - used;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < left; i += gridDim.x * blockDim.x)
+      R.freed_next[nfn + i] = R.freed_prev[used + i];
+  }
 }
 
-// Start of a round: locate the next stratum once the current one has thinned
-// to a quarter, stop when nothing is left, reset the per-round counters.
-__global__ void k_begin(Dev D) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// Start of a round (device side, one thread): locate the next stratum once
+// the current one has thinned to 1/2^overlap_shift of its size, stop when
+// nothing is left, reset the per-round counters.
+__device__ void begin_round(const Dev& D) {
   State* S = D.st;
   if (S->done || S->stop) return;
   S->act_total = 0;
@@ -1519,21 +1583,17 @@ __global__ void k_begin(Dev D) {
   C->n_inserted = 0;
   C->huge_used = 0;
   C->btab_used = 0;
+  C->work[0] = C->work[1] = C->work[2] = C->work[3] = 0;
 }
 
-// Recycled slots that were not handed out this round carry over.
-__global__ void k_carry(Dev D) {
-  const RoundArgs R = load_round(D);
-  if (!R.live) return;
-  const uint32_t used = __ldcg(&D.ctr->alloc_used);
-  const uint32_t nfn = __ldcg(&D.ctr->n_freed_next);
-  if (R.n_freed_prev <= used) return;
-  const uint32_t left = R.n_freed_prev - used;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < left; i += gridDim.x * blockDim.x)
-    R.freed_next[nfn + i] = R.freed_prev[used + i];
+// The first round's start (later rounds are started by k_end).
+__global__ void k_begin(Dev D) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  begin_round(D);
 }
 
-// End of a round: advance the slot top, swap the lists, stop on errors.
+// End of a round: advance the slot top, swap the lists, stop on errors; then
+// start the next round, so that a round is one kernel shorter.
 __global__ void k_end(Dev D) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   State* S = D.st;
@@ -1546,13 +1606,24 @@ __global__ void k_end(Dev D) {
   const uint32_t used = C->alloc_used;
   const uint32_t fresh = used > S->n_freed_prev ? used - S->n_freed_prev : 0u;
   const uint32_t left = S->n_freed_prev > used ? S->n_freed_prev - used : 0u;
-  S->tet_top += fresh;
+  // Winners that ran out of capacity reserved slot ranges they never wrote;
+  // every written slot lies below the capacity, so the top never passes it
+  // (the slots between are left dead).
+  S->tet_top = uint32_t(min(uint64_t(S->tet_top) + fresh, uint64_t(D.cap)));
   S->n_freed_prev = C->n_freed_next + left;
   S->par ^= 1u;
   S->n_active = C->n_next;
   S->inserted += C->n_inserted;
   S->starts += C->big_used + min(C->huge_used, HUGE_SLOTS);
-  if (C->err & kErrCapacity) S->stop = 2;
+  S->last_starts = C->big_used;
+  S->last_cand = C->n_cand;
+  S->last_inserted = C->n_inserted;
+  S->last_alloc = C->alloc_used;
+  if (C->err & kErrCapacity) {
+    S->stop = 2;
+    return;
+  }
+  begin_round(D);
 }
 
 // --------------------------------------------------------------- output ----
@@ -1745,7 +1816,7 @@ struct Workspace {
   DBuf<uint8_t> dup;
   DBuf<uint32_t> tcount, log_slot;
   DBuf<uint8_t> losses;
-  DBuf<uint8_t> ring2;
+  DBuf<uint8_t> ring2, prio;
   std::vector<DBuf<uint32_t>> scan_tmp;
   Counters* h_ctr = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -1824,7 +1895,7 @@ void release_thread_workspace() {
   w.ccount.release(); w.hullcnt.release(); w.cfill.release(); w.newid.release();
   w.hull.release(); w.coff.release(); w.out_t.release(); w.out_a.release(); w.dtab.release(); w.dup.release();
   w.etab_key.release(); w.etab_val.release(); w.btab_key.release(); w.btab_val.release();
-  w.tcount.release(); w.log_slot.release(); w.losses.release(); w.ring2.release();
+  w.tcount.release(); w.log_slot.release(); w.losses.release(); w.ring2.release(); w.prio.release();
   for (auto& b : w.scan_tmp) b.release();
   if (w.h_ctr) cudaFreeHost(w.h_ctr);
   if (w.ev0) cudaEventDestroy(w.ev0);
@@ -2109,7 +2180,11 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   if (vmode == 1) {
     W.ring2.reserve(nv, "pre-claim radius");
     ck(cudaMemsetAsync(W.ring2.p, 0, nv, s), "memset");
+    W.prio.reserve(nv, "claim priority");
+    ck(cudaMemsetAsync(W.prio.p, 0, nv, s), "memset");
   }
+  const char* sm_env = getenv("WTET_SCHED");
+  const uint32_t sched_mode = sm_env ? uint32_t(atoi(sm_env)) : 1u;
 
   Dev D{};
   auto refresh = [&]() {
@@ -2132,6 +2207,8 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     D.losses = vmode ? W.losses.p : nullptr;
     D.mlp = mlp_w;
     D.ring2 = vmode == 1 ? W.ring2.p : nullptr;
+    D.prio = vmode == 1 ? W.prio.p : nullptr;
+    D.sched_mode = sched_mode;
     D.deep_threshold = (cfg.deep_threshold ? float(cfg.deep_threshold) : 64.f) / 256.f;
     D.log_x = job.d_log_x;
     D.log_y = job.d_log_y;
@@ -2212,10 +2289,11 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   const uint32_t g_act = wave(k_activate, TB), g_tc = wave(k_tcount, TB), g_vote = wave(k_vote, TB);
   const uint32_t g_cand = wave(k_cands, TB), g_sched = wave(k_sched, 128), g_logf = wave(k_log_features, TB);
   const uint32_t g_bfs = wave(k_bfs, 128), g_res = wave(k_resolve, 128), g_sh = wave(k_shared, 128);
-  const uint32_t g_al = wave(k_alloc, 128), g_wr = wave(k_write, 128), g_rel = wave(k_relocate, TB);
+  const uint32_t g_wr = wave(k_write, 128), g_rel = wave(k_relocate, TB);
+  const uint64_t kernels_per_round = 10 + (vmode ? 2 : 0);
 
+  // One round: k_end also starts the next round (k_begin starts the first).
   auto enqueue_round = [&]() {
-    k_begin<<<1, 32, 0, s>>>(D);
     k_activate<<<g_act, TB, 0, s>>>(D);
     if (vmode) k_tcount<<<g_tc, TB, 0, s>>>(D);
     k_vote<<<g_vote, TB, 0, s>>>(D);
@@ -2226,10 +2304,8 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     k_expand_big<<<GB, 256, 0, s>>>(D);
     k_resolve<<<g_res, 128, 0, s>>>(D);
     k_shared<<<g_sh, 128, 0, s>>>(D);
-    k_alloc<<<g_al, 128, 0, s>>>(D);
     k_write<<<g_wr, 128, 0, s>>>(D);
     k_relocate<<<g_rel, TB, 0, s>>>(D);
-    k_carry<<<148, TB, 0, s>>>(D);
     k_end<<<1, 32, 0, s>>>(D);
   };
   // Rounds per host check (the graph holds this many rounds).
@@ -2247,6 +2323,8 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     cudaGraphDestroy(g);
   };
   build_graph();
+  k_begin<<<1, 32, 0, s>>>(D);
+  launches += 1;
   State hs{};
   cudaEvent_t tr0 = nullptr, tr1 = nullptr;  // per-round device time when tracing
   if (trace) {
@@ -2257,7 +2335,7 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     if (trace) ck(cudaEventRecord(tr0, s), "event record");
     ck(cudaGraphLaunch(gexec, s), "graph launch");
     if (trace) ck(cudaEventRecord(tr1, s), "event record");
-    launches += uint64_t(rpg) * (13 + (vmode ? 2 : 0));
+    launches += uint64_t(rpg) * kernels_per_round;
     ck(cudaMemcpyAsync(&hs, W.state.p, sizeof(State), cudaMemcpyDeviceToHost, s), "d2h");
     ck(cudaMemcpyAsync(W.h_ctr, W.ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, s), "d2h");
     ck(cudaStreamSynchronize(s), "rounds");
@@ -2268,8 +2346,8 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
       fprintf(stderr,
               "[wtet] round %u active %u winners %u expanded %llu cand %u inserted %u big %llu alloc %u top %u "
               "err %x ms %.3f\n",
-              hs.round, hs.n_active, h.big_used, (unsigned long long)h.n_expanded, h.n_cand, h.n_inserted,
-              (unsigned long long)h.n_big, h.alloc_used, hs.tet_top, h.err, rms);
+              hs.round, hs.n_active, hs.last_starts, (unsigned long long)h.n_expanded, hs.last_cand,
+              hs.last_inserted, (unsigned long long)h.n_big, hs.last_alloc, hs.tet_top, h.err, rms);
     }
     if (hs.stop == 1) {
       if (gexec) cudaGraphExecDestroy(gexec);
@@ -2314,6 +2392,8 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
       ck(cudaMemcpyAsync(&W.ctr.p->err, &zero, 4, cudaMemcpyHostToDevice, s), "clear err");
       ck(cudaStreamSynchronize(s), "grow");
       build_graph();
+      k_begin<<<1, 32, 0, s>>>(D);  // the stopped round did not start its successor
+      launches += 1;
       continue;
     }
     if (hs.done) break;
