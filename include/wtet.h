@@ -214,6 +214,16 @@ int wtet_check_quality_noalloc(const float* d_xyz, uint64_t n, const uint32_t* d
                                const uint32_t* d_adjacency, uint64_t m, uint64_t* violations,
                                uint64_t* interior_tets, void* stream);
 
+/* Signs of the device predicates as the insertion rounds evaluate them (FP32
+ * stage, FP64 filter, exact expansion stage, SoS), for testing them against
+ * other implementations of src/predicates.rs: for record i (points
+ * pts[15i..15i+14] as five xyz triples a..e, used as given, and SoS keys
+ * keys[5i..5i+4]) out3[i] = orient3d_sos(a,b,c,d) (+1 iff Shewchuk's
+ * orient3d < 0, src/predicates.rs:106-217) and out4[i] = orient4d(a,b,c,d,e)
+ * (sign of Shewchuk's insphere, SoS when 0: -1 = e inside,
+ * src/predicates.rs:450-675).  Host buffers. */
+int wtet_predicate_signs(const float* pts, const uint32_t* keys, uint64_t m, int32_t* out3, int32_t* out4);
+
 /* ---- Learned insertion scheduler (no counterpart in the reference, which
  * orders insertions by the circumsphere determinant alone,
  * src/shaders/vote.wgsl:401-494).  Every tet votes for its point deepest in

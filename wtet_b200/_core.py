@@ -108,6 +108,7 @@ EXPORTS = (
     "wtet_verify_device",
     "wtet_canonicalize",
     "wtet_canonicalize_device",
+    "wtet_predicate_signs",
 )
 
 
@@ -211,6 +212,8 @@ def load():
     L.wtet_canonicalize.restype = ctypes.c_int
     L.wtet_canonicalize_device.argtypes = [P, P, u64, u64, P, P, ctypes.POINTER(u64), P]
     L.wtet_canonicalize_device.restype = ctypes.c_int
+    L.wtet_predicate_signs.argtypes = [P, P, u64, P, P]
+    L.wtet_predicate_signs.restype = ctypes.c_int
     _lib = L
     _install_packaged_table()
     return L
@@ -553,6 +556,21 @@ def canonical_digest(canon_tets, canon_adjacency) -> str:
             arr = arr.cpu().numpy()
         h.update(np.ascontiguousarray(arr).view(np.uint32).astype("<u4", copy=False).tobytes())
     return h.hexdigest()
+
+
+def predicate_signs(points5, keys5):
+    """(orient3d_sos of the first four points, orient4d of all five) per
+    record, as the device's insertion rounds evaluate them: points5 (m, 5, 3)
+    float32 used as given, keys5 (m, 5) uint32 SoS keys."""
+    p = np.ascontiguousarray(points5, np.float32).reshape(-1, 15)
+    k = np.ascontiguousarray(keys5, np.uint32).reshape(-1, 5)
+    m = p.shape[0]
+    o3 = np.empty(m, np.int32)
+    o4 = np.empty(m, np.int32)
+    rc = load().wtet_predicate_signs(_ptr(p), _ptr(k), m, _ptr(o3), _ptr(o4))
+    if rc != WTET_OK:
+        _raise(rc)
+    return o3, o4
 
 
 def decode_adjacency(packed: int):

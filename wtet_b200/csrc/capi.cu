@@ -318,6 +318,32 @@ int wtet_canonicalize(const uint32_t* tets, const uint32_t* adjacency, uint64_t 
   }
 }
 
+int wtet_predicate_signs(const float* pts, const uint32_t* keys, uint64_t m, int32_t* out3, int32_t* out4) {
+  if (m && (!pts || !keys || !out3 || !out4)) return fail(WTET_ERR_ARG, "null pointer argument");
+  try {
+    require_device();
+    cudaStream_t s = nullptr;
+    // records, keys and both outputs in the per-thread input buffer
+    float* d = wtet::ws_input(15 * m + 5 * m + 2 * m + 16);
+    uint32_t* d_keys = reinterpret_cast<uint32_t*>(d + 15 * m);
+    int32_t* d_o3 = reinterpret_cast<int32_t*>(d + 20 * m);
+    int32_t* d_o4 = d_o3 + m;
+    if (m) {
+      ck(cudaMemcpyAsync(d, pts, 15 * m * 4, cudaMemcpyHostToDevice, s), "copy points");
+      ck(cudaMemcpyAsync(d_keys, keys, 5 * m * 4, cudaMemcpyHostToDevice, s), "copy keys");
+    }
+    wtet::predicate_signs_device(d, d_keys, m, d_o3, d_o4, s);
+    if (m) {
+      ck(cudaMemcpyAsync(out3, d_o3, m * 4, cudaMemcpyDeviceToHost, s), "copy signs");
+      ck(cudaMemcpyAsync(out4, d_o4, m * 4, cudaMemcpyDeviceToHost, s), "copy signs");
+    }
+    ck(cudaStreamSynchronize(s), "synchronize");
+    return WTET_OK;
+  } catch (const wtet::Error& e) {
+    return fail(e.status, e.msg);
+  }
+}
+
 void wtet_result_free(wtet_result* r) {
   if (!r) return;
   std::free(r->tets);

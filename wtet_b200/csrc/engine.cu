@@ -81,6 +81,11 @@ constexpr uint32_t HUGE_SLOTS = 64;
 constexpr uint8_t kPending = 0x80;
 constexpr uint8_t kDup = 0x40;  // exact duplicate of an earlier point: never inserted
 constexpr uint32_t WALK_LIMIT = 1u << 22;
+// The start list is bucketed by the top bits of each winner's claim hash, so
+// that the cavity search takes better-keyed winners first: a winner that
+// meets a better one's claims then stops at its first contested tet instead
+// of completing a cavity it loses later.
+constexpr uint32_t kOrderBuckets = 16;
 constexpr int ROT_LIMIT = 1 << 16;
 constexpr int kMaxLevels = 15;
 
@@ -105,7 +110,8 @@ struct Counters {
   uint32_t n_inserted;    // winners this round
   uint32_t huge_used;     // huge-cavity slots used
   uint32_t btab_used;     // k_write's large edge tables handed out this round
-  uint32_t work[4];       // dynamic work cursors of k_bfs, k_shared, k_write, k_resolve
+  uint32_t work[4];       // dynamic work cursors of k_bfs, k_shared, k_write (one spare)
+  uint32_t sbc[kOrderBuckets + 1];  // starts per order bucket (the last: overflow region)
   uint32_t err;           // error flags
   unsigned long long walk_steps;
   unsigned long long n_expanded;
@@ -162,6 +168,7 @@ struct Dev {
   unsigned long long* ccav;
   unsigned long long* cring;
   uint4* nslot;
+  uint32_t* bface;  // boundary faces of this round's winners, (tet << 2) | face, by allocation index
   unsigned long long* vote;
   uint32_t cap;
   uint32_t nv;  // vertices (range guard)
@@ -176,7 +183,10 @@ struct Dev {
   uint8_t* st1;  // candidate owns its whole cavity
   uint8_t* st2;  // ... and no shared face with a better winner is violated
   uint32_t* bigcand;  // points taking the huge-cavity path this round
-  uint32_t* starts;   // vote winners expanding their cavity this round
+  uint32_t* starts;   // vote winners expanding their cavity this round, in order-bucket regions
+  uint32_t start_rc;  // capacity of one order bucket's region
+  uint32_t start_ovf; // offset of the overflow region
+  uint32_t order_on;  // bucket the starts by claim hash
   unsigned long long* pre;  // neighbourhood pre-claims of the candidates
   uint32_t prefilter;
   uint32_t* wscratch; // one BIG_CAP cavity queue per lane group of k_bfs
@@ -196,8 +206,6 @@ struct Dev {
   uint8_t* losses;          // vote wins of each point that did not insert
   const mlp::Image* mlp;    // inference weights
   uint8_t* ring2;           // learned scheduler: the winner pre-claims two rings of neighbours
-  uint8_t* prio;            // learned scheduler: claim priority class of each winner (smaller first)
-  uint32_t sched_mode;      // learned scheduler: bit 0 ring radius from the score, bit 1 priority class
   float deep_threshold;     // learned scheduler: predicted probability above which it does
   float* log_x;             // logged features (log_cap x 12)
   uint8_t* log_y;           // logged labels: the winner inserted this round
@@ -277,17 +285,20 @@ __device__ __forceinline__ uint32_t mix32(uint32_t h) {
 // they would wait until their whole neighbourhood is quiet.  Every other
 // candidate has priority 1.
 __device__ __forceinline__ unsigned long long make_key(const Dev& D, const RoundArgs& R, uint32_t p) {
-  const unsigned long long prio = D.bigflag[p] == 2 ? 0u : 1u + (D.prio ? D.prio[p] : 0u);
+  const unsigned long long prio = D.bigflag[p] == 2 ? 0u : 1u;
   return R.stamp | (prio << 32) | mix32(p ^ (R.round * 0x9E3779B9u));
 }
 
 // Next work item of a warp-per-item kernel (dynamic: items differ widely in
 // cost, so warps that finish early take more).
-__device__ __forceinline__ uint32_t warp_next(uint32_t* cursor) {
+__device__ __forceinline__ uint32_t warp_next(uint32_t* cursor, uint32_t chunk) {
   uint32_t v = 0;
-  if ((threadIdx.x & 31) == 0) v = atomicAdd(cursor, 1u);
+  if ((threadIdx.x & 31) == 0) v = atomicAdd(cursor, chunk);
   return __shfl_sync(0xFFFFFFFFu, v, 0);
 }
+// Items are taken kChunk at a time: one shared cursor serves every warp of
+// the grid, and same-address atomics serialise in their L2 slice.
+constexpr uint32_t kChunk = 4;
 
 // Appends `pred` lanes to a list through one atomic per warp.
 __device__ __forceinline__ uint32_t warp_append(uint32_t* ctr, bool pred) {
@@ -320,32 +331,57 @@ __device__ __forceinline__ int o4d_sos(const double* a, const double* b, const d
   return ex::orient4d_sos_degenerate(A, B, C, Dd, E, sos[va], sos[vb], sos[vc], sos[vd], sos[ve], err);
 }
 
+// The same predicates on f32 points: the FP32 stage inline (it answers all
+// but a tiny fraction of tests), the FP64 filter, exact stage and SoS out of
+// line, so that the round kernels keep few registers live.
+__device__ __noinline__ int o3d_sos_slow(float4 a, float4 b, float4 c, float4 d, uint32_t va, uint32_t vb,
+                                         uint32_t vc, uint32_t vd, const uint32_t* sos, uint32_t* err) {
+  const double A[3] = {a.x, a.y, a.z}, B[3] = {b.x, b.y, b.z}, C[3] = {c.x, c.y, c.z}, Dd[3] = {d.x, d.y, d.z};
+  return o3d_sos(A, B, C, Dd, va, vb, vc, vd, sos, err);
+}
+__device__ __forceinline__ int o3d_sos_f(const float4& a, const float4& b, const float4& c, const float4& d,
+                                         uint32_t va, uint32_t vb, uint32_t vc, uint32_t vd, const uint32_t* sos,
+                                         uint32_t* err) {
+  const int s = ex::orient3d_f32(a, b, c, d);
+  if (s != 0) return s < 0 ? 1 : -1;
+  return o3d_sos_slow(a, b, c, d, va, vb, vc, vd, sos, err);
+}
+__device__ __noinline__ int o4d_sos_slow(float4 a, float4 b, float4 c, float4 d, float4 e, uint32_t va,
+                                         uint32_t vb, uint32_t vc, uint32_t vd, uint32_t ve, const uint32_t* sos,
+                                         uint32_t* err) {
+  const double A[3] = {a.x, a.y, a.z}, B[3] = {b.x, b.y, b.z}, C[3] = {c.x, c.y, c.z}, Dd[3] = {d.x, d.y, d.z};
+  const double E[3] = {e.x, e.y, e.z};
+  return o4d_sos(A, B, C, Dd, E, va, vb, vc, vd, ve, sos, err);
+}
+__device__ __forceinline__ int o4d_sos_f(const float4& a, const float4& b, const float4& c, const float4& d,
+                                         const float4& e, uint32_t va, uint32_t vb, uint32_t vc, uint32_t vd,
+                                         uint32_t ve, const uint32_t* sos, uint32_t* err) {
+  const int s = ex::insphere_f32(a, b, c, d, e);
+  if (s != 0) return s;
+  return o4d_sos_slow(a, b, c, d, e, va, vb, vc, vd, ve, sos, err);
+}
+
 // Visibility walk with exact orient3d + SoS from tet t to the tet containing p.
-__device__ __forceinline__ uint32_t walk_to(const Dev& D, uint32_t t, uint32_t p, const double* pp, uint32_t& steps) {
+__device__ __forceinline__ uint32_t walk_to(const Dev& D, uint32_t t, uint32_t p, const float4& pq, uint32_t& steps) {
   int entry = -1;
   for (uint32_t s = 0; s < WALK_LIMIT; ++s) {
     if (t >= D.cap) {
       atomicOr(&D.ctr->err, kErrGuard);
       return 0;
     }
-    uint4 V = D.tv[t];
+    const uint4 V = D.tv[t];
     if (V.x >= D.nv || V.y >= D.nv || V.z >= D.nv || V.w >= D.nv) {
       atomicOr(&D.ctr->err, kErrGuard);
       return t;
     }
-    uint32_t vv[4] = {V.x, V.y, V.z, V.w};
-    double P[4][3];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) load_pt(D.pts, vv[k], P[k]);
+    const float4 P0 = D.pts[V.x], P1 = D.pts[V.y], P2 = D.pts[V.z], P3 = D.pts[V.w];
     int moved = -1;
     for (int i = 0; i < 4; ++i) {
-      int f = (i + int(s)) & 3;
+      const int f = (i + int(s)) & 3;
       if (f == entry) continue;
-      const double* q[4] = {P[0], P[1], P[2], P[3]};
-      uint32_t w[4] = {vv[0], vv[1], vv[2], vv[3]};
-      q[f] = pp;
-      w[f] = p;
-      if (o3d_sos(q[0], q[1], q[2], q[3], w[0], w[1], w[2], w[3], D.sos, &D.ctr->err) == -1) {
+      // the tet with vertex f replaced by p
+      if (o3d_sos_f(f == 0 ? pq : P0, f == 1 ? pq : P1, f == 2 ? pq : P2, f == 3 ? pq : P3, f == 0 ? p : V.x,
+                    f == 1 ? p : V.y, f == 2 ? p : V.z, f == 3 ? p : V.w, D.sos, &D.ctr->err) == -1) {
         moved = f;
         break;
       }
@@ -354,7 +390,7 @@ __device__ __forceinline__ uint32_t walk_to(const Dev& D, uint32_t t, uint32_t p
       steps += s + 1;
       return t;
     }
-    uint32_t n = comp(D.tn[t], moved);
+    const uint32_t n = comp(D.tn[t], moved);
     if (n == NONE) {
       atomicOr(&D.ctr->err, kErrWalk);
       return t;
@@ -601,9 +637,7 @@ __global__ void __launch_bounds__(512, 2) k_activate(Dev D) {
       }
     }
     if (t == NONE) t = D.centry[c];
-    double pp[3];
-    load_pt(D.pts, p, pp);
-    D.loc[p] = walk_to(D, t, p, pp, steps);
+    D.loc[p] = walk_to(D, t, p, D.pts[p], steps);
     D.bigflag[p] = 0;
   }
   if (steps) atomicAdd(&D.ctr->walk_steps, (unsigned long long)steps);
@@ -655,6 +689,31 @@ __global__ void k_vote(Dev D) {
     unsigned long long key = ((unsigned long long)__float_as_uint(sc) << 32) | (unsigned long long)(~p);
     atomicMax(&D.vote[t], key);
   }
+}
+
+// Prefix of the order buckets' start counts, in shared memory (sp has
+// kOrderBuckets + 2 entries; sp[kOrderBuckets + 1] is the total).  Called by
+// every thread of the block.
+__device__ __forceinline__ void load_start_prefix(const Dev& D, uint32_t* sp) {
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (uint32_t b = 0; b <= kOrderBuckets; ++b) {
+      sp[b] = acc;
+      const uint32_t c = __ldcg(&D.ctr->sbc[b]);
+      acc += b < kOrderBuckets ? min(c, D.start_rc) : c;
+    }
+    sp[kOrderBuckets + 1] = acc;
+  }
+  __syncthreads();
+}
+
+// Start i of the round in bucket order.
+__device__ __forceinline__ uint32_t start_at(const Dev& D, const uint32_t* sp, uint32_t i) {
+  uint32_t b = 0;
+#pragma unroll
+  for (uint32_t k = 1; k <= kOrderBuckets; ++k) b += i >= sp[k] ? 1u : 0u;
+  const uint32_t region = b < kOrderBuckets ? b * D.start_rc : D.start_ovf;
+  return D.starts[region + (i - sp[b])];
 }
 
 // Uninserted points per tet for the learned scheduler and its log
@@ -751,10 +810,11 @@ __global__ void __launch_bounds__(128) k_sched(Dev D) {
   __shared__ __align__(16) mlp::Smem S;
   __shared__ __align__(16) uint32_t rows[4][32 * RS];
   __shared__ float outs[4][32];
+  __shared__ uint32_t sp[kOrderBuckets + 2];
   mlp::load_image(S, D.mlp);
-  __syncthreads();
+  load_start_prefix(D, sp);
   const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t nstart = __ldcg(&D.ctr->big_used);
+  const uint32_t nstart = sp[kOrderBuckets + 1];
   const uint32_t warps = gridDim.x * (blockDim.x >> 5);
   for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + w) * 32; base < nstart; base += warps * 32) {
     const uint32_t i = base + lane;
@@ -764,7 +824,7 @@ __global__ void __launch_bounds__(128) k_sched(Dev D) {
 #pragma unroll
     for (int k = 0; k < mlp::kIn; ++k) f[k] = 0.f;
     if (valid) {
-      p = D.starts[i];
+      p = start_at(D, sp, i);
       t = D.loc[p];
       winner_features(D, R, p, t, D.tv[t], f);
     }
@@ -774,10 +834,8 @@ __global__ void __launch_bounds__(128) k_sched(Dev D) {
     if (valid) {
       float sc = outs[w][lane];
       sc = (sc == sc) ? fminf(fmaxf(sc, -20.f), 20.f) : -20.f;
-      const float prob = 1.f / (1.f + __expf(-sc));
-      const bool two = (D.sched_mode & 1u) && prob > D.deep_threshold;
+      const bool two = 1.f / (1.f + __expf(-sc)) > D.deep_threshold;
       D.ring2[p] = two ? 1 : 0;
-      if (D.prio) D.prio[p] = (D.sched_mode & 2u) ? uint8_t(min(3, int(prob * 4.f))) : 0;
       if (D.prefilter) pre_claim(D, t, make_key(D, R, p), two);
     }
     __syncwarp();
@@ -789,9 +847,11 @@ __global__ void __launch_bounds__(128) k_sched(Dev D) {
 __global__ void k_log_features(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
-  const uint32_t nstart = __ldcg(&D.ctr->big_used);
+  __shared__ uint32_t sp[kOrderBuckets + 2];
+  load_start_prefix(D, sp);
+  const uint32_t nstart = sp[kOrderBuckets + 1];
   for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nstart; s += gridDim.x * blockDim.x) {
-    const uint32_t p = D.starts[s];
+    const uint32_t p = start_at(D, sp, s);
     uint32_t slot = NONE;
     const bool keep = (mix32(p ^ (R.round * 0x27D4EB2Fu)) & ((1u << D.log_shift) - 1u)) == 0u;
     if (keep) {
@@ -853,8 +913,22 @@ __global__ void k_cands(Dev D) {
         }
       }
     }
-    const uint32_t slot = warp_append(&D.ctr->big_used, start);
-    if (start) D.starts[slot] = p;
+    warp_append(&D.ctr->big_used, start);  // total count
+    const uint32_t b = (start && D.order_on) ? (mix32(p ^ (R.round * 0x9E3779B9u)) >> 28) : 0u;
+    const unsigned grp = __match_any_sync(0xFFFFFFFFu, start ? b : 0xFFFFFFFFu);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t leader = uint32_t(__ffs(grp) - 1);
+    uint32_t base = 0;
+    if (start && lane == leader) base = atomicAdd(&D.ctr->sbc[b], uint32_t(__popc(grp)));
+    base = __shfl_sync(0xFFFFFFFFu, base, int(leader));
+    if (start) {
+      const uint32_t slot = base + uint32_t(__popc(grp & ((1u << lane) - 1u)));
+      if (slot < D.start_rc) {
+        D.starts[b * D.start_rc + slot] = p;
+      } else {  // a bucket beyond its region (never expected): the overflow region
+        D.starts[D.start_ovf + atomicAdd(&D.ctr->sbc[kOrderBuckets], 1u)] = p;
+      }
+    }
   }
 }
 
@@ -901,27 +975,27 @@ __global__ void __launch_bounds__(128, 8) k_bfs(Dev D) {
   uint32_t* sq = sq_all[threadIdx.x / kBfsLanes];
   uint4* sn = sn_all[threadIdx.x / kBfsLanes];
   uint32_t* cav = D.wscratch + size_t(gid) * BIG_CAP;
-  const uint32_t nstart = __ldcg(&D.ctr->big_used);
-  // Work is taken dynamically, kWarpGroups consecutive starts per warp:
-  // cavities differ in size by orders of magnitude, and a static grid-stride
-  // split leaves warps idle behind the slowest ones.
-  for (;;) {
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(&D.ctr->work[0], kWarpGroups);
-    base = __shfl_sync(FULL, base, 0);
-    if (base >= nstart) break;  // warp-uniform
+  __shared__ uint32_t sp[kOrderBuckets + 2];
+  load_start_prefix(D, sp);
+  const uint32_t nstart = sp[kOrderBuckets + 1];
+  // Work is taken dynamically, kChunk x kWarpGroups consecutive starts per
+  // warp: cavities differ in size by orders of magnitude, and a static
+  // grid-stride split leaves warps idle behind the slowest ones.
+  for (uint32_t chunk0 = warp_next(&D.ctr->work[0], kWarpGroups * kChunk); chunk0 < nstart;
+       chunk0 = warp_next(&D.ctr->work[0], kWarpGroups * kChunk))
+  for (uint32_t base = chunk0; base < min(chunk0 + kWarpGroups * kChunk, nstart); base += kWarpGroups) {
     const uint32_t si = base + lane / kBfsLanes;
     bool active = si < nstart;
     uint32_t p = 0, t0 = 0;
     if (active) {
-      p = D.starts[si];
+      p = start_at(D, sp, si);
       t0 = D.loc[p];
     }
     unsigned long long key = 0;
-    double pp[3] = {0.0, 0.0, 0.0};
+    float4 pq = make_float4(0.f, 0.f, 0.f, 0.f);
     if (active) {
       key = make_key(D, R, p);
-      load_pt(D.pts, p, pp);
+      pq = D.pts[p];
     }
     int pre_lost = 0;
     if (active && D.prefilter) {
@@ -972,12 +1046,8 @@ __global__ void __launch_bounds__(128, 8) k_bfs(Dev D) {
               if (W.x >= D.nv || W.y >= D.nv || W.z >= D.nv || W.w >= D.nv) {
                 my_guard = true;
               } else {
-                double P[4][3];
-                load_pt(D.pts, W.x, P[0]);
-                load_pt(D.pts, W.y, P[1]);
-                load_pt(D.pts, W.z, P[2]);
-                load_pt(D.pts, W.w, P[3]);
-                const int sg = o4d_sos(P[0], P[1], P[2], P[3], pp, W.x, W.y, W.z, W.w, p, D.sos, &D.ctr->err);
+                const int sg = o4d_sos_f(D.pts[W.x], D.pts[W.y], D.pts[W.z], D.pts[W.w], pq, W.x, W.y, W.z, W.w, p,
+                                         D.sos, &D.ctr->err);
                 if (sg < 0) {
                   const unsigned long long old = atomicMin(&D.ccav[nt], key);
                   if (old < key) my_lost = true;
@@ -1072,8 +1142,7 @@ __global__ void __launch_bounds__(256) k_expand_big(Dev D) {
   const uint32_t t0 = D.loc[p];
   uint32_t* cav = big_slot(D, bi);
   const unsigned long long key = make_key(D, R, p);
-  double pp[3];
-  load_pt(D.pts, p, pp);
+  const float4 pq = D.pts[p];
   if (tid == 0) {
     D.st1[p] = 0;
     D.st2[p] = 0;
@@ -1105,12 +1174,8 @@ __global__ void __launch_bounds__(256) k_expand_big(Dev D) {
           if (W.x >= D.nv || W.y >= D.nv || W.z >= D.nv || W.w >= D.nv) {
             sGuard = 1u;
           } else {
-            double P[4][3];
-            load_pt(D.pts, W.x, P[0]);
-            load_pt(D.pts, W.y, P[1]);
-            load_pt(D.pts, W.z, P[2]);
-            load_pt(D.pts, W.w, P[3]);
-            const int sg = o4d_sos(P[0], P[1], P[2], P[3], pp, W.x, W.y, W.z, W.w, p, D.sos, &D.ctr->err);
+            const int sg = o4d_sos_f(D.pts[W.x], D.pts[W.y], D.pts[W.z], D.pts[W.w], pq, W.x, W.y, W.z, W.w, p,
+                                     D.sos, &D.ctr->err);
             if (sg < 0) {
               const unsigned long long old = atomicMin(&D.ccav[nt], key);
               if (old < key) {
@@ -1153,7 +1218,8 @@ __global__ void k_resolve(Dev D) {
   if (!R.live) return;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t ncand = __ldcg(&D.ctr->n_cand);
-  for (uint32_t ci = warp_next(&D.ctr->work[3]); ci < ncand; ci = warp_next(&D.ctr->work[3])) {
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ci < ncand; ci += nwarps) {
     uint32_t p = D.cand[ci];
     uint32_t K = D.cand_len[ci];
     const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
@@ -1199,7 +1265,8 @@ __global__ void __launch_bounds__(128, 8) k_shared(Dev D) {
   constexpr uint32_t FULL = 0xFFFFFFFFu;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t ncand = __ldcg(&D.ctr->n_cand);
-  for (uint32_t ci = warp_next(&D.ctr->work[1]); ci < ncand; ci = warp_next(&D.ctr->work[1])) {
+  for (uint32_t c0 = warp_next(&D.ctr->work[1], kChunk); c0 < ncand; c0 = warp_next(&D.ctr->work[1], kChunk))
+  for (uint32_t ci = c0; ci < min(c0 + kChunk, ncand); ++ci) {
     const uint32_t p = D.cand[ci];
     if (!D.st1[p]) {
       if (lane == 0) D.st2[p] = 0;
@@ -1208,8 +1275,6 @@ __global__ void __launch_bounds__(128, 8) k_shared(Dev D) {
     const uint32_t K = D.cand_len[ci];
     const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
     const unsigned long long key = make_key(D, R, p);
-    double pp[3];
-    load_pt(D.pts, p, pp);
     // one lane per (cavity tet, face): boundary faces are counted (their
     // flags kept in a register for cavities of up to 64 tets), faces shared
     // with a better winner are tested
@@ -1227,17 +1292,12 @@ __global__ void __launch_bounds__(128, 8) k_shared(Dev D) {
         if (bnd && nb != NONE && !bad && cc < key && this_round(R, cc)) {
           const uint32_t q = key_owner(R, cc);
           if (q < D.nv && D.st1[q]) {
+            // the new tet on face f: p replaces vertex f
             const uint4 V = D.tv[c];
-            uint32_t w[4];
-            double P[4][3];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {  // the new tet on face f: p replaces vertex f
-              w[k] = k == f ? p : comp(V, k);
-              load_pt(D.pts, w[k], P[k]);
-            }
-            double qq[3];
-            load_pt(D.pts, q, qq);
-            if (o4d_sos(P[0], P[1], P[2], P[3], qq, w[0], w[1], w[2], w[3], q, D.sos, &D.ctr->err) < 0) bad = true;
+            const uint32_t w0 = f == 0 ? p : V.x, w1 = f == 1 ? p : V.y, w2 = f == 2 ? p : V.z, w3 = f == 3 ? p : V.w;
+            if (o4d_sos_f(D.pts[w0], D.pts[w1], D.pts[w2], D.pts[w3], D.pts[q], w0, w1, w2, w3, q, D.sos,
+                          &D.ctr->err) < 0)
+              bad = true;
           }
         }
       }
@@ -1278,9 +1338,9 @@ __global__ void __launch_bounds__(128, 8) k_shared(Dev D) {
         }
       }
       const uint32_t ball = __ballot_sync(FULL, bnd);
-      if (e < 4 * K)
-        reinterpret_cast<uint32_t*>(D.nslot + c)[f] =
-            bnd ? slot_of(D, R, base + run + __popc(ball & ((1u << lane) - 1u))) : NONE;
+      const uint32_t v = base + run + __popc(ball & ((1u << lane) - 1u));
+      if (e < 4 * K) reinterpret_cast<uint32_t*>(D.nslot + c)[f] = bnd ? slot_of(D, R, v) : NONE;
+      if (bnd) D.bface[v] = (c << 2) | uint32_t(f);
       run += __popc(ball);
     }
     if (lane == 0) {
@@ -1321,13 +1381,15 @@ __global__ void __launch_bounds__(128, 8) k_write(Dev D) {
   const uint32_t w = threadIdx.x >> 5;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t ncand = __ldcg(&D.ctr->n_cand);
-  for (uint32_t ci = warp_next(&D.ctr->work[2]); ci < ncand; ci = warp_next(&D.ctr->work[2])) {
+  for (uint32_t c0 = warp_next(&D.ctr->work[2], kChunk); c0 < ncand; c0 = warp_next(&D.ctr->work[2], kChunk))
+  for (uint32_t ci = c0; ci < min(c0 + kChunk, ncand); ++ci) {
     uint32_t p = D.cand[ci];
     if (!D.st2[p]) continue;
     uint32_t K = D.cand_len[ci];
     const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
     unsigned long long key = make_key(D, R, p);
     const uint32_t F = D.cand_nf[ci];  // boundary faces, counted by k_shared
+    const uint32_t vbase = D.cand_base[ci];  // their allocation (virtual slot) indices
     unsigned long long* tk = nullptr;
     uint32_t *t0 = nullptr, *t1 = nullptr;
     uint32_t mask = 31;
@@ -1358,11 +1420,11 @@ __global__ void __launch_bounds__(128, 8) k_write(Dev D) {
         t1[j] = NONE;
       }
       __syncwarp();
-      for (uint32_t e = lane; e < 4 * K; e += 32) {
-        const uint32_t c = cav[e >> 2];
-        const int f = int(e & 3u);
-        const uint32_t sl = reinterpret_cast<const uint32_t*>(D.nslot + c)[f];
-        if (sl == NONE) continue;
+      for (uint32_t j = lane; j < F; j += 32) {
+        const uint32_t bf = D.bface[vbase + j];
+        const uint32_t c = bf >> 2;
+        const int f = int(bf & 3u);
+        const uint32_t sl = slot_of(D, R, vbase + j);
         const uint4 V = D.tv[c];
         {
           for (int k = 0; k < 4; ++k) {
@@ -1385,12 +1447,13 @@ __global__ void __launch_bounds__(128, 8) k_write(Dev D) {
       __syncwarp();
     }
     bool bad = false;
-    // one lane per (cavity tet, face): a boundary face becomes one new tet
-    for (uint32_t e = lane; e < 4 * K; e += 32) {
-      const uint32_t c = cav[e >> 2];
-      const int f = int(e & 3u);
-      const uint32_t sl = reinterpret_cast<const uint32_t*>(D.nslot + c)[f];
-      if (sl == NONE) continue;
+    // one lane per boundary face (the compact list k_shared wrote): each
+    // becomes one new tet
+    for (uint32_t j = lane; j < F; j += 32) {
+      const uint32_t bf = D.bface[vbase + j];
+      const uint32_t c = bf >> 2;
+      const int f = int(bf & 3u);
+      const uint32_t sl = slot_of(D, R, vbase + j);
       const uint4 V = D.tv[c];
       {
         uint32_t outer = reinterpret_cast<const uint32_t*>(D.tn + c)[f];
@@ -1470,7 +1533,7 @@ __global__ void __launch_bounds__(128, 8) k_write(Dev D) {
     }
     if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) atomicOr(&D.ctr->err, kErrRotate);
     __syncwarp();  // every lane is done reading the cavity before it is retired
-    const uint32_t s0 = slot_of(D, R, D.cand_base[ci]);
+    const uint32_t s0 = slot_of(D, R, vbase);
     uint32_t fbase = 0;
     if (lane == 0) fbase = atomicAdd(&D.ctr->n_freed_next, K);
     fbase = __shfl_sync(0xFFFFFFFFu, fbase, 0);
@@ -1522,11 +1585,7 @@ __global__ void __launch_bounds__(512, 2) k_relocate(Dev D) {
         keep = true;
         if (D.bigflag[p] & kPending) D.bigflag[p] &= uint8_t(~kPending);
         uint4 V = D.tv[t];
-        if (V.x == DEAD) {
-          double pp[3];
-          load_pt(D.pts, p, pp);
-          D.loc[p] = walk_to(D, V.y, p, pp, steps);
-        }
+        if (V.x == DEAD) D.loc[p] = walk_to(D, V.y, p, D.pts[p], steps);
       }
     }
     uint32_t slot = warp_append(&D.ctr->n_next, keep);
@@ -1584,6 +1643,7 @@ __device__ void begin_round(const Dev& D) {
   C->huge_used = 0;
   C->btab_used = 0;
   C->work[0] = C->work[1] = C->work[2] = C->work[3] = 0;
+  for (uint32_t b = 0; b <= kOrderBuckets; ++b) C->sbc[b] = 0;
 }
 
 // The first round's start (later rounds are started by k_end).
@@ -1624,6 +1684,24 @@ __global__ void k_end(Dev D) {
     return;
   }
   begin_round(D);
+}
+
+// ------------------------------------------------------ predicate check ----
+
+// Signs of the round kernels' predicates on given records of five points and
+// five SoS keys (testing only): orient3d_sos of the first four, orient4d of all
+// five, through the same FP32 stage / FP64 filter / exact / SoS chain.
+__global__ void k_predicate_signs(const float* pts, const uint32_t* keys, uint64_t m, int32_t* o3, int32_t* o4,
+                                  uint32_t* err) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x) {
+    const float* q = pts + 15 * i;
+    const float4 a = make_float4(q[0], q[1], q[2], 0.f), b = make_float4(q[3], q[4], q[5], 0.f);
+    const float4 c = make_float4(q[6], q[7], q[8], 0.f), d = make_float4(q[9], q[10], q[11], 0.f);
+    const float4 e = make_float4(q[12], q[13], q[14], 0.f);
+    const uint32_t* k = keys + 5 * i;
+    o3[i] = o3d_sos_f(a, b, c, d, 0, 1, 2, 3, k, err);
+    o4[i] = o4d_sos_f(a, b, c, d, e, 0, 1, 2, 3, 4, k, err);
+  }
 }
 
 // --------------------------------------------------------------- output ----
@@ -1799,6 +1877,7 @@ struct Workspace {
   DBuf<uint32_t> sos, vcloud, vtet, loc;
   DBuf<uint8_t> bigflag;
   DBuf<uint4> tv, tn, nslot;
+  DBuf<uint32_t> bface;
   DBuf<unsigned long long> ccav, cring, vote, pre;
   DBuf<uint32_t> centry, active, active_next, cand, cand_off, cand_len, cand_base, cand_nf, pool, big, freed_a, freed_b;
   DBuf<uint8_t> st1, st2;
@@ -1816,7 +1895,7 @@ struct Workspace {
   DBuf<uint8_t> dup;
   DBuf<uint32_t> tcount, log_slot;
   DBuf<uint8_t> losses;
-  DBuf<uint8_t> ring2, prio;
+  DBuf<uint8_t> ring2;
   std::vector<DBuf<uint32_t>> scan_tmp;
   Counters* h_ctr = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -1888,14 +1967,14 @@ void release_thread_workspace() {
   w.xyz.release(); w.off.release(); w.ci.release(); w.mn.release(); w.mx.release();
   w.bucket.release(); w.hist.release(); w.tmp.release(); w.pts.release(); w.sos.release();
   w.vcloud.release(); w.vtet.release(); w.loc.release(); w.bigflag.release(); w.tv.release();
-  w.tn.release(); w.nslot.release(); w.ccav.release(); w.cring.release(); w.pre.release(); w.vote.release();
+  w.tn.release(); w.nslot.release(); w.bface.release(); w.ccav.release(); w.cring.release(); w.pre.release(); w.vote.release();
   w.centry.release(); w.active.release(); w.active_next.release(); w.cand.release();
   w.cand_off.release(); w.cand_len.release(); w.cand_base.release(); w.cand_nf.release(); w.st1.release(); w.st2.release(); w.bigcand.release(); w.starts.release(); w.wscratch.release(); w.pool.release(); w.big.release();
   w.freed_a.release(); w.freed_b.release(); w.lvl_off.release(); w.lvl_total.release(); w.state.release(); w.ctr.release();
   w.ccount.release(); w.hullcnt.release(); w.cfill.release(); w.newid.release();
   w.hull.release(); w.coff.release(); w.out_t.release(); w.out_a.release(); w.dtab.release(); w.dup.release();
   w.etab_key.release(); w.etab_val.release(); w.btab_key.release(); w.btab_val.release();
-  w.tcount.release(); w.log_slot.release(); w.losses.release(); w.ring2.release(); w.prio.release();
+  w.tcount.release(); w.log_slot.release(); w.losses.release(); w.ring2.release();
   for (auto& b : w.scan_tmp) b.release();
   if (w.h_ctr) cudaFreeHost(w.h_ctr);
   if (w.ev0) cudaEventDestroy(w.ev0);
@@ -2122,7 +2201,11 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   W.cand_nf.reserve(n, "cand");
   W.st1.reserve(nv, "status");
   W.bigcand.reserve(HUGE_SLOTS, "bigcand");
-  W.starts.reserve(n, "starts");
+  const char* ord_env = getenv("WTET_ORDER");
+  const uint32_t order_on = ord_env ? uint32_t(atoi(ord_env) != 0) : 1u;
+  const uint64_t start_rc = order_on ? (n / kOrderBuckets + n / 64 + 1024) : n;
+  const uint64_t start_ovf = order_on ? start_rc * kOrderBuckets : n;
+  W.starts.reserve(start_ovf + n, "starts");
   // one overflow queue per lane group of a k_bfs wave
   W.wscratch.reserve(size_t(wave(k_bfs, 128)) * (128 / kBfsLanes) * BIG_CAP, "cavity queues");
   const uint32_t etab_warps = wave(k_write, 128) * 4;  // one edge table per warp of a k_write wave
@@ -2148,6 +2231,7 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     W.tv.reserve(cap, "tv");
     W.tn.reserve(cap, "tn");
     W.nslot.reserve(cap, "nslot");
+    W.bface.reserve(cap, "boundary faces");
     W.ccav.reserve(cap, "ccav");
     W.cring.reserve(cap, "cring");
     W.pre.reserve(cap, "pre");
@@ -2180,20 +2264,17 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   if (vmode == 1) {
     W.ring2.reserve(nv, "pre-claim radius");
     ck(cudaMemsetAsync(W.ring2.p, 0, nv, s), "memset");
-    W.prio.reserve(nv, "claim priority");
-    ck(cudaMemsetAsync(W.prio.p, 0, nv, s), "memset");
   }
-  const char* sm_env = getenv("WTET_SCHED");
-  const uint32_t sched_mode = sm_env ? uint32_t(atoi(sm_env)) : 1u;
 
   Dev D{};
   auto refresh = [&]() {
     D.pts = W.pts.p; D.sos = W.sos.p; D.vcloud = W.vcloud.p; D.vtet = W.vtet.p; D.loc = W.loc.p;
     D.bigflag = W.bigflag.p; D.tv = W.tv.p; D.tn = W.tn.p; D.ccav = W.ccav.p; D.cring = W.cring.p;
-    D.nslot = W.nslot.p; D.vote = W.vote.p; D.cap = uint32_t(cap); D.nv = uint32_t(nv); D.centry = W.centry.p;
+    D.nslot = W.nslot.p; D.bface = W.bface.p; D.vote = W.vote.p; D.cap = uint32_t(cap); D.nv = uint32_t(nv); D.centry = W.centry.p;
     D.cand = W.cand.p; D.cand_off = W.cand_off.p;
     D.cand_len = W.cand_len.p; D.cand_base = W.cand_base.p; D.cand_nf = W.cand_nf.p; D.st1 = W.st1.p; D.st2 = W.st2.p; D.bigcand = W.bigcand.p;
     D.starts = W.starts.p; D.wscratch = W.wscratch.p; D.pre = W.pre.p;
+    D.start_rc = uint32_t(start_rc); D.start_ovf = uint32_t(start_ovf); D.order_on = order_on;
     D.etab_key = W.etab_key.p; D.etab_val = W.etab_val.p; D.etab_warps = etab_warps;
     D.btab_key = W.btab_key.p; D.btab_val = W.btab_val.p;
     D.prefilter = cfg.candidate_filter == 2 ? 0u : 1u; D.pool = W.pool.p; D.pool_cap = pool_cap; D.big = W.big.p;
@@ -2207,8 +2288,6 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     D.losses = vmode ? W.losses.p : nullptr;
     D.mlp = mlp_w;
     D.ring2 = vmode == 1 ? W.ring2.p : nullptr;
-    D.prio = vmode == 1 ? W.prio.p : nullptr;
-    D.sched_mode = sched_mode;
     D.deep_threshold = (cfg.deep_threshold ? float(cfg.deep_threshold) : 64.f) / 256.f;
     D.log_x = job.d_log_x;
     D.log_y = job.d_log_y;
@@ -2368,6 +2447,7 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
       ck(cudaMemsetAsync(W.tv.p + top, 0xFF, (ncap - top) * sizeof(uint4), s), "memset");
       W.tn.grow_keep(ncap, top, s, "grow tn");
       W.nslot.grow_keep(ncap, 0, s, "grow nslot");
+      W.bface.grow_keep(ncap, 0, s, "grow boundary faces");
       W.ccav.grow_keep(ncap, top, s, "grow ccav");
       ck(cudaMemsetAsync(W.ccav.p + top, 0xFF, (ncap - top) * 8, s), "memset");
       W.cring.grow_keep(ncap, top, s, "grow cring");
@@ -2569,6 +2649,19 @@ void check_quality_device(const float* d_xyz, uint64_t n, const uint32_t* d_tets
   if (W.h_ctr->err & kErrPrec) throw Error{WTET_ERR_PRECISION, "exact arithmetic buffer overflow"};
   *violations = W.h_ctr->walk_steps;
   *interior = W.h_ctr->n_expanded;
+}
+
+void predicate_signs_device(const float* d_pts, const uint32_t* d_keys, uint64_t m, int32_t* d_o3, int32_t* d_o4,
+                            cudaStream_t s) {
+  Workspace& W = ws();
+  W.ctr.reserve(1, "counters");
+  ck(cudaMemsetAsync(W.ctr.p, 0, sizeof(Counters), s), "memset");
+  if (m) k_predicate_signs<<<blocks_for(m, 128, 148 * 8), 128, 0, s>>>(d_pts, d_keys, m, d_o3, d_o4, &W.ctr.p->err);
+  ck(cudaGetLastError(), "predicate kernel");
+  uint32_t err = 0;
+  ck(cudaMemcpyAsync(&err, &W.ctr.p->err, 4, cudaMemcpyDeviceToHost, s), "d2h");
+  ck(cudaStreamSynchronize(s), "predicates");
+  if (err) throw Error{WTET_ERR_PRECISION, "exact arithmetic buffer overflow"};
 }
 
 }  // namespace wtet

@@ -68,6 +68,10 @@ uint64_t canonicalize_device(const uint32_t* d_tets, const uint32_t* d_adj, uint
                              uint32_t* d_out_tets, uint32_t* d_out_adj, cudaStream_t stream);
 void release_verify_workspace();
 
+// Signs of the round kernels' predicates on records of five points (testing).
+void predicate_signs_device(const float* d_pts, const uint32_t* d_keys, uint64_t m, int32_t* d_o3, int32_t* d_o4,
+                            cudaStream_t stream);
+
 // Upper bound on output tets for a cloud of n points.
 uint64_t max_tets_for(uint64_t n);
 

@@ -6,6 +6,14 @@
 //   orient3d_sos                src/predicates.rs:106-208
 //   orient4d (insphere + SoS)   src/predicates.rs:450-675
 //
+// An FP32 stage may run ahead of the FP64 filter (insphere_f32 /
+// orient3d_f32): the same determinant and permanent in single precision with
+// Shewchuk's stage-A bound for unit roundoff 2^-24.  Those bounds hold for any
+// IEEE precision as long as nothing underflows, so the stage answers only when
+// the permanent is far above the smallest normal float (and the values are
+// finite); it returns 0 -- "not certain" -- otherwise, and the FP64 filter,
+// the exact stage and SoS decide as before.  It never changes a sign.
+//
 // Coordinates are f32 values widened to f64.  The exact stage evaluates the
 // determinants from raw coordinates (4x4 / 5x5 with a column of ones, expanded
 // by cofactors), so it needs no exact coordinate differences.  The SoS
@@ -335,6 +343,87 @@ __device__ __forceinline__ int insphere(const double* pa, const double* pb, cons
   double c[3] = {pc[0], pc[1], pc[2]}, d[3] = {pd[0], pd[1], pd[2]};
   double e[3] = {pe[0], pe[1], pe[2]};
   return insphere_exact_sign(a, b, c, d, e, flags);
+}
+
+// ---- FP32 stage ----
+
+constexpr float kEpsF = 5.9604644775390625e-08f;  // 2^-24
+constexpr float kO3dBoundF = (7.0f + 56.0f * kEpsF) * kEpsF;
+constexpr float kIspBoundF = (16.0f + 224.0f * kEpsF) * kEpsF;
+// Permanents below this get no answer (typical permanents of the benchmark
+// clouds are above 1e-16).
+constexpr float kPermMinF = 1.0e-26f;
+// Absolute slack added to the bound for gradual underflow: each of the ~60
+// operations may lose at most 2^-150 to a subnormal result, which reaches the
+// determinant multiplied by at most 500 * 7.5e5 (coordinate differences within
+// the super tetrahedron's extent of 500, lifted terms below 7.5e5): < 2e-35 in
+// all.  At the smallest permanent answered the bound itself is ~1e-32.
+constexpr float kUnderflowSlackF = 1.0e-33f;
+
+// Sign of Shewchuk orient3d(a,b,c,d) when certain from f32 arithmetic, else 0.
+__device__ __forceinline__ int orient3d_f32(const float4& pa, const float4& pb, const float4& pc,
+                                            const float4& pd) {
+  const float adx = __fsub_rn(pa.x, pd.x), bdx = __fsub_rn(pb.x, pd.x), cdx = __fsub_rn(pc.x, pd.x);
+  const float ady = __fsub_rn(pa.y, pd.y), bdy = __fsub_rn(pb.y, pd.y), cdy = __fsub_rn(pc.y, pd.y);
+  const float adz = __fsub_rn(pa.z, pd.z), bdz = __fsub_rn(pb.z, pd.z), cdz = __fsub_rn(pc.z, pd.z);
+  const float bdxcdy = __fmul_rn(bdx, cdy), cdxbdy = __fmul_rn(cdx, bdy);
+  const float cdxady = __fmul_rn(cdx, ady), adxcdy = __fmul_rn(adx, cdy);
+  const float adxbdy = __fmul_rn(adx, bdy), bdxady = __fmul_rn(bdx, ady);
+  const float det = __fadd_rn(__fadd_rn(__fmul_rn(adz, __fsub_rn(bdxcdy, cdxbdy)),
+                                        __fmul_rn(bdz, __fsub_rn(cdxady, adxcdy))),
+                              __fmul_rn(cdz, __fsub_rn(adxbdy, bdxady)));
+  const float perm = __fadd_rn(__fadd_rn(__fmul_rn(__fadd_rn(fabsf(bdxcdy), fabsf(cdxbdy)), fabsf(adz)),
+                                         __fmul_rn(__fadd_rn(fabsf(cdxady), fabsf(adxcdy)), fabsf(bdz))),
+                               __fmul_rn(__fadd_rn(fabsf(adxbdy), fabsf(bdxady)), fabsf(cdz)));
+  if (!(perm >= kPermMinF && perm < 1.0e30f)) return 0;
+  const float err = __fadd_rn(__fmul_rn(kO3dBoundF, perm), kUnderflowSlackF);
+  if (det > err) return 1;
+  if (-det > err) return -1;
+  return 0;
+}
+
+// Sign of Shewchuk insphere(a,b,c,d,e) when certain from f32 arithmetic, else 0.
+__device__ __forceinline__ int insphere_f32(const float4& pa, const float4& pb, const float4& pc, const float4& pd,
+                                            const float4& pe) {
+  const float aex = __fsub_rn(pa.x, pe.x), bex = __fsub_rn(pb.x, pe.x);
+  const float cex = __fsub_rn(pc.x, pe.x), dex = __fsub_rn(pd.x, pe.x);
+  const float aey = __fsub_rn(pa.y, pe.y), bey = __fsub_rn(pb.y, pe.y);
+  const float cey = __fsub_rn(pc.y, pe.y), dey = __fsub_rn(pd.y, pe.y);
+  const float aez = __fsub_rn(pa.z, pe.z), bez = __fsub_rn(pb.z, pe.z);
+  const float cez = __fsub_rn(pc.z, pe.z), dez = __fsub_rn(pd.z, pe.z);
+  const float aexbey = __fmul_rn(aex, bey), bexaey = __fmul_rn(bex, aey), ab = __fsub_rn(aexbey, bexaey);
+  const float bexcey = __fmul_rn(bex, cey), cexbey = __fmul_rn(cex, bey), bc = __fsub_rn(bexcey, cexbey);
+  const float cexdey = __fmul_rn(cex, dey), dexcey = __fmul_rn(dex, cey), cd = __fsub_rn(cexdey, dexcey);
+  const float dexaey = __fmul_rn(dex, aey), aexdey = __fmul_rn(aex, dey), da = __fsub_rn(dexaey, aexdey);
+  const float aexcey = __fmul_rn(aex, cey), cexaey = __fmul_rn(cex, aey), ac = __fsub_rn(aexcey, cexaey);
+  const float bexdey = __fmul_rn(bex, dey), dexbey = __fmul_rn(dex, bey), bd = __fsub_rn(bexdey, dexbey);
+  const float abc = __fadd_rn(__fsub_rn(__fmul_rn(aez, bc), __fmul_rn(bez, ac)), __fmul_rn(cez, ab));
+  const float bcd = __fadd_rn(__fsub_rn(__fmul_rn(bez, cd), __fmul_rn(cez, bd)), __fmul_rn(dez, bc));
+  const float cda = __fadd_rn(__fadd_rn(__fmul_rn(cez, da), __fmul_rn(dez, ac)), __fmul_rn(aez, cd));
+  const float dab = __fadd_rn(__fadd_rn(__fmul_rn(dez, ab), __fmul_rn(aez, bd)), __fmul_rn(bez, da));
+  const float alift = __fadd_rn(__fadd_rn(__fmul_rn(aex, aex), __fmul_rn(aey, aey)), __fmul_rn(aez, aez));
+  const float blift = __fadd_rn(__fadd_rn(__fmul_rn(bex, bex), __fmul_rn(bey, bey)), __fmul_rn(bez, bez));
+  const float clift = __fadd_rn(__fadd_rn(__fmul_rn(cex, cex), __fmul_rn(cey, cey)), __fmul_rn(cez, cez));
+  const float dlift = __fadd_rn(__fadd_rn(__fmul_rn(dex, dex), __fmul_rn(dey, dey)), __fmul_rn(dez, dez));
+  const float det = __fadd_rn(__fsub_rn(__fmul_rn(dlift, abc), __fmul_rn(clift, dab)),
+                              __fsub_rn(__fmul_rn(blift, cda), __fmul_rn(alift, bcd)));
+  const float az = fabsf(aez), bz = fabsf(bez), cz = fabsf(cez), dz = fabsf(dez);
+  const float p_ab = __fadd_rn(fabsf(aexbey), fabsf(bexaey)), p_bc = __fadd_rn(fabsf(bexcey), fabsf(cexbey));
+  const float p_cd = __fadd_rn(fabsf(cexdey), fabsf(dexcey)), p_da = __fadd_rn(fabsf(dexaey), fabsf(aexdey));
+  const float p_ac = __fadd_rn(fabsf(aexcey), fabsf(cexaey)), p_bd = __fadd_rn(fabsf(bexdey), fabsf(dexbey));
+  const float t_a = __fadd_rn(__fadd_rn(__fmul_rn(p_cd, bz), __fmul_rn(p_bd, cz)), __fmul_rn(p_bc, dz));
+  const float t_b = __fadd_rn(__fadd_rn(__fmul_rn(p_da, cz), __fmul_rn(p_ac, dz)), __fmul_rn(p_cd, az));
+  const float t_c = __fadd_rn(__fadd_rn(__fmul_rn(p_ab, dz), __fmul_rn(p_bd, az)), __fmul_rn(p_da, bz));
+  const float t_d = __fadd_rn(__fadd_rn(__fmul_rn(p_bc, az), __fmul_rn(p_ac, bz)), __fmul_rn(p_ab, cz));
+  // summed in Shewchuk's order: ((a + b) + c) + d
+  const float perm = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(t_a, alift), __fmul_rn(t_b, blift)),
+                                         __fmul_rn(t_c, clift)),
+                               __fmul_rn(t_d, dlift));
+  if (!(perm >= kPermMinF && perm < 1.0e30f)) return 0;
+  const float err = __fadd_rn(__fmul_rn(kIspBoundF, perm), kUnderflowSlackF);
+  if (det > err) return 1;
+  if (-det > err) return -1;
+  return 0;
 }
 
 // ---- SoS cascade pieces (src/predicates.rs) ----
