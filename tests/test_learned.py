@@ -141,8 +141,11 @@ def test_collect_records(gpu):
     X, y, st = learned.collect([pts], sample_shift=0)
     assert 0 < X.shape[0] == y.shape[0] <= st["vote_winners"]
     assert np.isfinite(X).all()
-    assert set(np.unique(y)) == {0, 1}
+    assert set(np.unique(y)) == {0, 1}                     # inserted in its round, or not
     assert (X[:, 0] >= 0).all() and (X[:, 0] <= 1).all()   # circumcenter distance
+    assert (X[:, 6] >= 0).all() and (X[:, 6] < 1).all()    # claim priority
+    assert (X[:, 7] > 0).all() and (X[:, 7] <= 1).all()    # a better winner reaches the second ring
+    assert (X[:, 7] <= X[:, 4]).all()                      # better winners are among all winners there
     assert (X[:, 8] >= 0).all() and (X[:, 8] <= 1).all()   # rival neighbours / 4
     assert set(np.unique(X[:, 11])) <= {0.0, 1.0}          # super-vertex flag
 
@@ -160,10 +163,10 @@ def test_learned_scheduler_parity(gpu, oracle_mod, name):
 
 
 @pytest.mark.gpu
-def test_trained_network_predicts_large_cavities(gpu):
-    """What the trained network gains over knowing nothing: on records logged
-    from clouds it was not trained on, its predictions of a large cavity beat
-    the base rate (lower cross-entropy, AUC well above chance)."""
+def test_trained_network_predicts_insertions(gpu):
+    """What the trained network knows: on records logged from clouds it was
+    not trained on, its prediction of which gated winners insert beats the
+    base rate (lower cross-entropy, AUC well above chance)."""
     from wtet_b200 import learned
 
     learned.load_default()
@@ -174,27 +177,26 @@ def test_trained_network_predicts_large_cavities(gpu):
         bce = np.mean(np.logaddexp(0, logit) - y * logit)
         q = y.mean()
         base = -(q * np.log(q) + (1 - q) * np.log(1 - q))
-        order = np.argsort(logit, kind="stable")
-        ranks = np.empty(len(logit))
-        ranks[order] = np.arange(1, len(logit) + 1)
-        pos = y > 0.5
-        auc = (ranks[pos].sum() - pos.sum() * (pos.sum() + 1) / 2) / (pos.sum() * (~pos).sum())
-        print(f"records {len(y)} large {q:.3f} bce {bce:.4f} base-rate entropy {base:.4f} auc {auc:.3f}")
-        assert bce < base - 0.02
-        assert auc > 0.7
+        auc = learned.roc_auc(logit, y)
+        print(f"records {len(y)} inserted {q:.3f} bce {bce:.4f} base-rate entropy {base:.4f} auc {auc:.3f}")
+        assert bce < base - 0.01
+        assert auc > 0.65
 
 
 @pytest.mark.gpu
 def test_learned_scheduler_gain(gpu):
-    """What the learned scheduler gains over the plain one, on the degenerate
-    lattice configuration (large cospherical cavities): the same tet set in
-    less device time (median of three runs each) and fewer cavity searches."""
+    """What the learned scheduler gains over the plain one on the degenerate
+    lattice configuration (large cospherical cavities, where a lost cavity
+    search is expensive): the same tet set, far fewer cavity searches and less
+    device time (median of five runs each, interleaved)."""
     pts = fx.lattice(96)
     cfg_plain, cfg_learned = gpu.Config(), gpu.Config(vote="learned")
     gpu.delaunay(pts, cfg_plain)
     gpu.delaunay(pts, cfg_learned)
-    plain = [gpu.delaunay(pts, cfg_plain) for _ in range(3)]
-    learned = [gpu.delaunay(pts, cfg_learned) for _ in range(3)]
+    plain, learned = [], []
+    for _ in range(5):
+        plain.append(gpu.delaunay(pts, cfg_plain))
+        learned.append(gpu.delaunay(pts, cfg_learned))
 
     def canon(t):
         s = np.sort(t.astype(np.int64), axis=1)
@@ -207,5 +209,5 @@ def test_learned_scheduler_gain(gpu):
         st = r.stats
         print(f"{name}: {t:.1f} ms, rounds {st['rounds']}, winners {st['vote_winners']}, "
               f"cavity searches {st['candidates']}")
-    assert learned[0].stats["candidates"] < plain[0].stats["candidates"]
+    assert learned[0].stats["candidates"] < 0.7 * plain[0].stats["candidates"]
     assert tl < tp

@@ -2,8 +2,12 @@
 
 ``python -m wtet_b200.build`` compiles the CUDA sources in ``csrc/`` with
 nvcc for ``arch=compute_100a,code=sm_100a`` into ``wtet_b200/libwtet.so``
-(in-tree, so the library travels with the repository).  ``-fmad=false`` is
-required: the exact predicates rely on separately rounded products and sums.
+(in-tree, so the library travels with the repository).  Each source is its
+own object, compiled in parallel.  The sources that evaluate the exact
+predicates (EXACT_SOURCES) are compiled with ``-fmad=false``: the filters,
+expansions and the reference's SoS arithmetic rely on separately rounded
+products and sums.  The others (the scheduler network's training and scoring
+kernels, the C ABI) keep FMA contraction.
 """
 from __future__ import annotations
 
@@ -18,16 +22,16 @@ LIB = os.path.join(HERE, "libwtet.so")
 SOURCES = ["engine.cu", "capi.cu", "noalloc.cu", "learned.cu", "verify.cu"]
 HEADERS = ["exact.cuh", "engine.cuh", "learned.cuh", "order.cuh", "devbuf.cuh"]
 
+EXACT_SOURCES = {"engine.cu", "verify.cu", "noalloc.cu"}
+
 NVCC_FLAGS = [
     "-O3",
     "-std=c++17",
     "-gencode",
     "arch=compute_100a,code=sm_100a",
     "-lineinfo",
-    "-fmad=false",
     "-Xcompiler",
     "-fPIC",
-    "-shared",
     "-diag-suppress",
     "177,550",
 ]
@@ -56,14 +60,35 @@ def up_to_date() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return LIB
-    cmd = [nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-o", LIB + ".tmp"] + sources()
-    r = subprocess.run(cmd, capture_output=True, text=True)
-    if r.returncode != 0:
-        sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed building libwtet.so")
-    if verbose:
-        sys.stderr.write(r.stderr)
-    os.replace(LIB + ".tmp", LIB)
+    import concurrent.futures as cf
+    import tempfile
+
+    tmp = tempfile.mkdtemp(prefix="wtet_build_")
+
+    def compile_one(src):
+        obj = os.path.join(tmp, os.path.basename(src) + ".o")
+        flags = NVCC_FLAGS + (["-fmad=false"] if os.path.basename(src) in EXACT_SOURCES else [])
+        cmd = [nvcc()] + flags + (["-Xptxas", "-v"] if verbose else []) + ["-c", src, "-o", obj]
+        return obj, subprocess.run(cmd, capture_output=True, text=True)
+
+    try:
+        with cf.ThreadPoolExecutor(len(sources())) as ex:
+            results = list(ex.map(compile_one, sources()))
+        failed = False
+        for obj, r in results:
+            if r.returncode != 0 or verbose:
+                sys.stderr.write(r.stdout + r.stderr)
+            failed = failed or r.returncode != 0
+        if failed:
+            raise RuntimeError("nvcc failed building libwtet.so")
+        link = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB + ".tmp"]
+        r = subprocess.run(link + [o for o, _ in results], capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("nvcc failed linking libwtet.so")
+        os.replace(LIB + ".tmp", LIB)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
     return LIB
 
 

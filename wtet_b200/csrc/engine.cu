@@ -13,15 +13,15 @@
 // SoS Delaunay triangulation, with no flip failures and nothing left to repair.
 //
 // Round structure (one insertion round over all clouds of a job; 10 kernels
-// replayed from a CUDA graph, 12 with the learned scheduler):
+// replayed from a CUDA graph, 11 with the learned scheduler):
 //   k_activate    locate the new stratum's points (walk from the curve
 //                 predecessor's tet)
 //   k_vote        each uninserted point votes for its tet (64-bit atomicMax of
 //                 score | ~point, src/shaders/vote.wgsl semantics)
 //   k_cands       the winner of each tet becomes a candidate and pre-claims
 //                 its tet's neighbourhood with its claim key
-//   (k_tcount, k_sched: the learned scheduler sets each winner's pre-claim
-//                 radius from the fused BF16 MLP instead)
+//   (k_sched      the learned scheduler decides which winners search this
+//                 round, with the fused BF16 MLP)
 //   k_bfs         candidates whose pre-claims all hold grow their cavities by
 //                 breadth-first search with exact insphere (16 lanes per
 //                 candidate), claiming cavity tets by 64-bit atomicMin of a
@@ -110,6 +110,7 @@ struct Counters {
   uint32_t n_inserted;    // winners this round
   uint32_t huge_used;     // huge-cavity slots used
   uint32_t btab_used;     // k_write's large edge tables handed out this round
+  uint32_t bface_used;    // boundary-face list entries this round
   uint32_t work[4];       // dynamic work cursors of k_bfs, k_shared, k_write (one spare)
   uint32_t sbc[kOrderBuckets + 1];  // starts per order bucket (the last: overflow region)
   uint32_t err;           // error flags
@@ -146,6 +147,23 @@ struct alignas(16) State {
   uint32_t last_starts, last_cand, last_inserted, last_alloc;
 };
 
+// One tet slot: its vertex ids (retired: {DEAD, forward}) and its links,
+// (neighbour << 2) | face, NONE on the super tetrahedron's hull -- one 32-byte
+// sector, so that a visit reads both with one memory transaction.
+struct __align__(32) Tet {
+  uint4 v;
+  uint4 n;
+};
+// The per-round words of one tet slot, likewise one sector: the cavity claim
+// (64-bit key, smallest wins), the "tested outside" memo of the cavity search,
+// the neighbourhood pre-claim and the vote (score | ~point).
+struct __align__(32) Claim {
+  unsigned long long cav;
+  unsigned long long ring;
+  unsigned long long pre;
+  unsigned long long vote;
+};
+
 // Everything a kernel needs, passed by value.
 struct Dev {
   State* st;
@@ -163,13 +181,11 @@ struct Dev {
   uint32_t* loc;     // containing tet of uninserted points; INS_BIT once inserted
   uint8_t* bigflag;  // point needs the large-cavity path
   // tets
-  uint4* tv;
-  uint4* tn;  // (tet << 2) | face, NONE on the super tetrahedron's hull
-  unsigned long long* ccav;
-  unsigned long long* cring;
+  Tet* T;
+  Claim* C;
   uint4* nslot;
-  uint32_t* bface;  // boundary faces of this round's winners, (tet << 2) | face, by allocation index
-  unsigned long long* vote;
+  uint32_t* bface;  // boundary faces of this round's winners, (tet << 2) | face, per winner contiguous
+  uint32_t inplace; // small stars reuse their cavity's slots
   uint32_t cap;
   uint32_t nv;  // vertices (range guard)
   // clouds
@@ -186,8 +202,7 @@ struct Dev {
   uint32_t* starts;   // vote winners expanding their cavity this round, in order-bucket regions
   uint32_t start_rc;  // capacity of one order bucket's region
   uint32_t start_ovf; // offset of the overflow region
-  uint32_t order_on;  // bucket the starts by claim hash
-  unsigned long long* pre;  // neighbourhood pre-claims of the candidates
+  uint32_t exp_order, exp_bchunk;
   uint32_t prefilter;
   uint32_t* wscratch; // one BIG_CAP cavity queue per lane group of k_bfs
   unsigned long long* etab_key;  // k_write's global edge tables, kEdgeSlotsG per warp
@@ -202,14 +217,13 @@ struct Dev {
   int rule;
   // learned scheduler (vote_mode 1) and its training log (vote_mode 2)
   uint32_t vote_mode;
-  uint32_t* tcount;         // uninserted points per tet this round
   uint8_t* losses;          // vote wins of each point that did not insert
   const mlp::Image* mlp;    // inference weights
-  uint8_t* ring2;           // learned scheduler: the winner pre-claims two rings of neighbours
-  float deep_threshold;     // learned scheduler: predicted probability above which it does
+  uint8_t* defer;           // learned scheduler: the winner waits for the next round
+  float deep_threshold;     // learned scheduler: predicted insert probability below which it does
   float* log_x;             // logged features (log_cap x 12)
-  uint8_t* log_y;           // logged labels: the winner inserted this round
-  uint32_t* log_slot;       // log record of each start, NONE if not sampled
+  uint8_t* log_y;           // logged labels: the winner inserted this round (1) or not (0)
+  uint32_t* log_pslot;      // log record of each winner this round, NONE if not recorded
   uint32_t log_cap;
   uint32_t log_shift;       // keep 1 in 2^log_shift winners
 };
@@ -299,6 +313,10 @@ __device__ __forceinline__ uint32_t warp_next(uint32_t* cursor, uint32_t chunk) 
 // Items are taken kChunk at a time: one shared cursor serves every warp of
 // the grid, and same-address atomics serialise in their L2 slice.
 constexpr uint32_t kChunk = 4;
+// Stars of at most this many tets are written into their own cavity's slots
+// (k_write holds one new tet per lane in registers until the warp has read
+// the whole cavity).
+constexpr uint32_t kInPlaceFaces = 32;
 
 // Appends `pred` lanes to a list through one atomic per warp.
 __device__ __forceinline__ uint32_t warp_append(uint32_t* ctr, bool pred) {
@@ -339,10 +357,11 @@ __device__ __noinline__ int o3d_sos_slow(float4 a, float4 b, float4 c, float4 d,
   const double A[3] = {a.x, a.y, a.z}, B[3] = {b.x, b.y, b.z}, C[3] = {c.x, c.y, c.z}, Dd[3] = {d.x, d.y, d.z};
   return o3d_sos(A, B, C, Dd, va, vb, vc, vd, sos, err);
 }
+__device__ int g_exp_f32 = 1;
 __device__ __forceinline__ int o3d_sos_f(const float4& a, const float4& b, const float4& c, const float4& d,
                                          uint32_t va, uint32_t vb, uint32_t vc, uint32_t vd, const uint32_t* sos,
                                          uint32_t* err) {
-  const int s = ex::orient3d_f32(a, b, c, d);
+  const int s = g_exp_f32 ? ex::orient3d_f32(a, b, c, d) : 0;
   if (s != 0) return s < 0 ? 1 : -1;
   return o3d_sos_slow(a, b, c, d, va, vb, vc, vd, sos, err);
 }
@@ -356,7 +375,7 @@ __device__ __noinline__ int o4d_sos_slow(float4 a, float4 b, float4 c, float4 d,
 __device__ __forceinline__ int o4d_sos_f(const float4& a, const float4& b, const float4& c, const float4& d,
                                          const float4& e, uint32_t va, uint32_t vb, uint32_t vc, uint32_t vd,
                                          uint32_t ve, const uint32_t* sos, uint32_t* err) {
-  const int s = ex::insphere_f32(a, b, c, d, e);
+  const int s = g_exp_f32 ? ex::insphere_f32(a, b, c, d, e) : 0;
   if (s != 0) return s;
   return o4d_sos_slow(a, b, c, d, e, va, vb, vc, vd, ve, sos, err);
 }
@@ -369,7 +388,7 @@ __device__ __forceinline__ uint32_t walk_to(const Dev& D, uint32_t t, uint32_t p
       atomicOr(&D.ctr->err, kErrGuard);
       return 0;
     }
-    const uint4 V = D.tv[t];
+    const uint4 V = D.T[t].v;
     if (V.x >= D.nv || V.y >= D.nv || V.z >= D.nv || V.w >= D.nv) {
       atomicOr(&D.ctr->err, kErrGuard);
       return t;
@@ -390,7 +409,7 @@ __device__ __forceinline__ uint32_t walk_to(const Dev& D, uint32_t t, uint32_t p
       steps += s + 1;
       return t;
     }
-    const uint32_t n = comp(D.tn[t], moved);
+    const uint32_t n = comp(D.T[t].n, moved);
     if (n == NONE) {
       atomicOr(&D.ctr->err, kErrWalk);
       return t;
@@ -571,6 +590,17 @@ __global__ void k_scatter_points(const uint64_t* off, const CloudInfo* ci, uint3
   D.vtet[v] = NONE;
 }
 
+// Unused tet slots: dead, no links; claims and pre-claims at the largest key
+// (any claim beats them), no vote.
+__global__ void k_init_slots(Tet* T, Claim* C, uint64_t from, uint64_t to) {
+  for (uint64_t i = from + uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < to;
+       i += uint64_t(gridDim.x) * blockDim.x) {
+    T[i].v = make_uint4(DEAD, DEAD, DEAD, DEAD);
+    T[i].n = make_uint4(NONE, NONE, NONE, NONE);
+    C[i] = Claim{~0ull, ~0ull, ~0ull, 0ull};
+  }
+}
+
 // Super vertices (src/gpu/mod.rs:151-158) and the initial super tet of every
 // cloud, oriented with orient3d_sos > 0 (src/phase2.rs:404-410).
 __global__ void k_init_clouds(const CloudInfo* ci, uint32_t nc, Dev D) {
@@ -590,8 +620,8 @@ __global__ void k_init_clouds(const CloudInfo* ci, uint32_t nc, Dev D) {
   double P[4][3];
   for (int k = 0; k < 4; ++k) load_pt(D.pts, s0 + k, P[k]);
   int o = o3d_sos(P[0], P[1], P[2], P[3], s0, s0 + 1, s0 + 2, s0 + 3, D.sos, &D.ctr->err);
-  D.tv[c] = (o > 0) ? make_uint4(s0, s0 + 1, s0 + 2, s0 + 3) : make_uint4(s0 + 1, s0, s0 + 2, s0 + 3);
-  D.tn[c] = make_uint4(NONE, NONE, NONE, NONE);
+  D.T[c].v = (o > 0) ? make_uint4(s0, s0 + 1, s0 + 2, s0 + 3) : make_uint4(s0 + 1, s0, s0 + 2, s0 + 3);
+  D.T[c].n = make_uint4(NONE, NONE, NONE, NONE);
   D.centry[c] = c;
 }
 
@@ -632,7 +662,7 @@ __global__ void __launch_bounds__(512, 2) k_activate(Dev D) {
       uint32_t hl = D.loc[hv];
       uint32_t h = (hl & INS_BIT) ? D.vtet[hv] : hl;
       if (h != NONE && h < D.cap) {
-        uint4 V = D.tv[h];
+        uint4 V = D.T[h].v;
         if (V.x < D.nv && D.vcloud[V.x] == c) t = h;
       }
     }
@@ -680,14 +710,14 @@ __global__ void k_vote(Dev D) {
       atomicOr(&D.ctr->err, kErrGuard);
       continue;
     }
-    uint4 V = D.tv[t];
+    uint4 V = D.T[t].v;
     if (V.x >= D.nv || V.y >= D.nv || V.z >= D.nv || V.w >= D.nv) {
       atomicOr(&D.ctr->err, kErrGuard);
       continue;
     }
     float sc = vote_score(D.pts, V, D.pts[p], D.rule);
     unsigned long long key = ((unsigned long long)__float_as_uint(sc) << 32) | (unsigned long long)(~p);
-    atomicMax(&D.vote[t], key);
+    atomicMax(&D.C[t].vote, key);
   }
 }
 
@@ -716,159 +746,6 @@ __device__ __forceinline__ uint32_t start_at(const Dev& D, const uint32_t* sp, u
   return D.starts[region + (i - sp[b])];
 }
 
-// Uninserted points per tet for the learned scheduler and its log
-// (warp-aggregated: Morton-ordered neighbours in the list usually share a
-// tet).  Every tet with a count holds a vote winner.  Reset by k_relocate.
-__global__ void k_tcount(Dev D) {
-  const RoundArgs R = load_round(D);
-  if (!R.live) return;
-  for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < R.n_active; i0 += gridDim.x * blockDim.x) {
-    const uint32_t i = i0 + threadIdx.x;
-    uint32_t t = NONE;
-    if (i < R.n_active) {
-      const uint32_t p = R.active[i];
-      if (!(D.bigflag[p] & kDup) && D.loc[p] < D.cap) t = D.loc[p];
-    }
-    const unsigned peers = __match_any_sync(0xFFFFFFFFu, t);
-    if (t != NONE && (threadIdx.x & 31) == uint32_t(__ffs(peers) - 1)) atomicAdd(&D.tcount[t], uint32_t(__popc(peers)));
-  }
-}
-
-// Features of vote winner p in its tet t (vertices V); k_cands has already
-// counted this win in losses[p].
-__device__ __forceinline__ void winner_features(const Dev& D, const RoundArgs& R, uint32_t p, uint32_t t, uint4 V,
-                                                float* f) {
-  const float4 q = D.pts[p];
-  const float depth = vote_score(D.pts, V, q, 0);
-  const CloudInfo C = D.ci[D.vcloud[p]];
-  const uint32_t pn = (p + 1 < C.vbase + C.n) ? p + 1 : p - 1;  // Morton neighbour in the same cloud
-  const float4 r = D.pts[pn];
-  const float dx = r.x - q.x, dy = r.y - q.y, dz = r.z - q.z;
-  const uint4 N = D.tn[t];
-  uint32_t rivals = 0;
-  float crowd = 0.f;
-#pragma unroll
-  for (int f = 0; f < 4; ++f) {
-    const uint32_t nb = comp(N, f);
-    if (nb == NONE || (nb >> 2) >= D.cap) continue;
-    const uint32_t c = D.tcount[nb >> 2];
-    rivals += c ? 1u : 0u;
-    crowd += __log2f(1.f + float(c));
-  }
-  const uint32_t lost = D.losses[p] ? D.losses[p] - 1u : 0u;
-  mlp::features(D.pts[V.x], D.pts[V.y], D.pts[V.z], D.pts[V.w], q, depth, D.tcount[t], lost, R.round,
-                sqrtf(dx * dx + dy * dy + dz * dz), rivals, crowd, f);
-}
-
-// Pre-claims of vote winner p in tet t with its key: t and its face
-// neighbours, and with `two` also the other neighbours of those (up to 17
-// tets).  A candidate whose pre-claimed tets are not all its own would lose its
-// cavity to a better one, so it skips cavity growth (k_bfs checks them).
-__device__ __forceinline__ void pre_claim(const Dev& D, uint32_t t, unsigned long long key, bool two) {
-  atomicMin(&D.pre[t], key);
-  const uint4 N = D.tn[t];
-  for (int f = 0; f < 4; ++f) {
-    const uint32_t nb = comp(N, f);
-    if (nb == NONE || (nb >> 2) >= D.cap) continue;
-    atomicMin(&D.pre[nb >> 2], key);
-    if (!two) continue;
-    const uint4 N2 = D.tn[nb >> 2];
-    for (int g = 1; g < 4; ++g) {  // the three faces other than the one back to t
-      const uint32_t nb2 = comp(N2, (int(nb & 3) + g) & 3);
-      if (nb2 != NONE && (nb2 >> 2) < D.cap) atomicMin(&D.pre[nb2 >> 2], key);
-    }
-  }
-}
-
-// Tet k of p's pre-claim set (k = 0: t; k = 1 + 4i: face neighbour i;
-// k = 1 + 4i + j, j = 1..3: the j-th other neighbour of face neighbour i), or
-// NONE.
-__device__ __forceinline__ uint32_t pre_claim_tet(const Dev& D, uint32_t t, uint32_t k) {
-  if (k == 0) return t;
-  const uint32_t i = (k - 1) / 4, j = (k - 1) % 4;
-  const uint32_t nb = comp(D.tn[t], int(i));
-  if (nb == NONE || (nb >> 2) >= D.cap) return NONE;
-  if (j == 0) return nb >> 2;
-  const uint32_t nb2 = comp(D.tn[nb >> 2], (int(nb & 3) + int(j)) & 3);
-  return (nb2 == NONE || (nb2 >> 2) >= D.cap) ? NONE : nb2 >> 2;
-}
-
-// Learned scheduler, after k_cands: the fused tensor-core MLP scores the
-// vote winners (32 per warp, consecutive in the start list) with the
-// predicted probability that the winner's cavity is large (more than
-// kLargeCavity tets).  Those winners pre-claim two rings of neighbours, the
-// others one: a large cavity conflicts with candidates the one-ring pre-claim
-// cannot see, and finding that out by a full (expensive) cavity search wastes
-// it, while pre-claiming two rings for every winner blocks many small
-// cavities that would not have met and costs rounds (measured: two rings
-// everywhere is 13% faster on the 2M lattice and 5-25% slower on the mixture
-// and the sphere).
-__global__ void __launch_bounds__(128) k_sched(Dev D) {
-  const RoundArgs R = load_round(D);
-  if (!R.live) return;
-  constexpr int RS = mlp::kRowStride;
-  __shared__ __align__(16) mlp::Smem S;
-  __shared__ __align__(16) uint32_t rows[4][32 * RS];
-  __shared__ float outs[4][32];
-  __shared__ uint32_t sp[kOrderBuckets + 2];
-  mlp::load_image(S, D.mlp);
-  load_start_prefix(D, sp);
-  const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t nstart = sp[kOrderBuckets + 1];
-  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-  for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + w) * 32; base < nstart; base += warps * 32) {
-    const uint32_t i = base + lane;
-    const bool valid = i < nstart;
-    uint32_t p = 0, t = 0;
-    float f[mlp::kIn];
-#pragma unroll
-    for (int k = 0; k < mlp::kIn; ++k) f[k] = 0.f;
-    if (valid) {
-      p = start_at(D, sp, i);
-      t = D.loc[p];
-      winner_features(D, R, p, t, D.tv[t], f);
-    }
-    mlp::stage_row(rows[w] + lane * RS, f);
-    __syncwarp();
-    mlp::score32(S, rows[w], outs[w]);
-    if (valid) {
-      float sc = outs[w][lane];
-      sc = (sc == sc) ? fminf(fmaxf(sc, -20.f), 20.f) : -20.f;
-      const bool two = 1.f / (1.f + __expf(-sc)) > D.deep_threshold;
-      D.ring2[p] = two ? 1 : 0;
-      if (D.prefilter) pre_claim(D, t, make_key(D, R, p), two);
-    }
-    __syncwarp();
-  }
-}
-
-// Scheduler log, after k_cands: features of 1 in 2^log_shift vote winners;
-// k_bfs fills in their labels.
-__global__ void k_log_features(Dev D) {
-  const RoundArgs R = load_round(D);
-  if (!R.live) return;
-  __shared__ uint32_t sp[kOrderBuckets + 2];
-  load_start_prefix(D, sp);
-  const uint32_t nstart = sp[kOrderBuckets + 1];
-  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nstart; s += gridDim.x * blockDim.x) {
-    const uint32_t p = start_at(D, sp, s);
-    uint32_t slot = NONE;
-    const bool keep = (mix32(p ^ (R.round * 0x27D4EB2Fu)) & ((1u << D.log_shift) - 1u)) == 0u;
-    if (keep) {
-      slot = atomicAdd(&D.st->log_used, 1u);
-      if (slot >= D.log_cap) slot = NONE;
-    }
-    D.log_slot[s] = slot;
-    if (slot == NONE) continue;
-    D.log_y[slot] = 255;  // unknown until k_bfs completes the winner's cavity
-    const uint32_t t = D.loc[p];
-    float f[mlp::kIn];
-    winner_features(D, R, p, t, D.tv[t], f);
-#pragma unroll
-    for (int k = 0; k < mlp::kIn; ++k) D.log_x[size_t(slot) * mlp::kIn + k] = f[k];
-  }
-}
-
 
 // Inverse of mix32: recovers the point that owns a claim key.
 __device__ __forceinline__ uint32_t unmix32(uint32_t h) {
@@ -886,6 +763,183 @@ __device__ __forceinline__ bool this_round(const RoundArgs& R, unsigned long lon
   return (key >> 48) == (R.stamp >> 48);
 }
 
+// Pre-claims of vote winner p in tet t with its key: t and its face
+// neighbours, and with `two` also the other neighbours of those (up to 17
+// tets).  A candidate whose pre-claimed tets are not all its own would lose its
+// cavity to a better one, so it skips cavity growth (k_bfs checks them).
+__device__ __forceinline__ void pre_claim(const Dev& D, uint32_t t, unsigned long long key, bool two) {
+  atomicMin(&D.C[t].pre, key);
+  const uint4 N = D.T[t].n;
+  for (int f = 0; f < 4; ++f) {
+    const uint32_t nb = comp(N, f);
+    if (nb == NONE || (nb >> 2) >= D.cap) continue;
+    atomicMin(&D.C[nb >> 2].pre, key);
+    if (!two) continue;
+    const uint4 N2 = D.T[nb >> 2].n;
+    for (int g = 1; g < 4; ++g) {  // the three faces other than the one back to t
+      const uint32_t nb2 = comp(N2, (int(nb & 3) + g) & 3);
+      if (nb2 != NONE && (nb2 >> 2) < D.cap) atomicMin(&D.C[nb2 >> 2].pre, key);
+    }
+  }
+}
+
+// Tet k of p's pre-claim set (k = 0: t; k = 1 + 4i: face neighbour i;
+// k = 1 + 4i + j, j = 1..3: the j-th other neighbour of face neighbour i), or
+// NONE.
+__device__ __forceinline__ uint32_t pre_claim_tet(const Dev& D, uint32_t t, uint32_t k) {
+  if (k == 0) return t;
+  const uint32_t i = (k - 1) / 4, j = (k - 1) % 4;
+  const uint32_t nb = comp(D.T[t].n, int(i));
+  if (nb == NONE || (nb >> 2) >= D.cap) return NONE;
+  if (j == 0) return nb >> 2;
+  const uint32_t nb2 = comp(D.T[nb >> 2].n, (int(nb & 3) + int(j)) & 3);
+  return (nb2 == NONE || (nb2 >> 2) >= D.cap) ? NONE : nb2 >> 2;
+}
+
+// Pre-claim state of vote winner p in tet t0 after k_cands: lost1 -- a better
+// winner overwrote one of p's own pre-claims (t0 and its face neighbours),
+// so the plain filter skips p this round; better2 / any2 -- tets of p's
+// second ring (the other neighbours of its face neighbours) that hold a
+// better / any winner's pre-claim of this round; rivals -- face neighbours
+// that hold a vote winner.  (A claim record holds the pre-claim and the vote
+// in one sector.)
+__device__ __forceinline__ void filter_state(const Dev& D, const RoundArgs& R, uint32_t t0, unsigned long long key,
+                                             bool& lost1, uint32_t& better2, uint32_t& any2, uint32_t& rivals) {
+  lost1 = false;
+  better2 = any2 = rivals = 0;
+  const uint4 N = D.T[t0].n;
+  uint32_t nbt[4];
+  if (__ldcg(&D.C[t0].pre) != key) lost1 = true;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint32_t nb = comp(N, i);
+    nbt[i] = (nb == NONE || (nb >> 2) >= D.cap) ? NONE : nb;
+    if (nbt[i] == NONE) continue;
+    const Claim* c1 = &D.C[nb >> 2];
+    if (__ldcg(&c1->pre) != key) lost1 = true;
+    if (__ldcg(&c1->vote) != 0ull) ++rivals;
+  }
+  if (lost1) return;  // the plain filter skips this winner: no decision to make
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint32_t nb = nbt[i];
+    if (nb == NONE) continue;
+    const uint4 N2 = D.T[nb >> 2].n;
+#pragma unroll
+    for (int g = 1; g < 4; ++g) {
+      const uint32_t nb2 = comp(N2, (int(nb & 3) + g) & 3);
+      if (nb2 == NONE || (nb2 >> 2) >= D.cap) continue;
+      const unsigned long long pv = __ldcg(&D.C[nb2 >> 2].pre);
+      if (this_round(R, pv)) {
+        ++any2;
+        if (pv < key) ++better2;
+      }
+    }
+  }
+}
+
+// Features of vote winner p in its tet t (vertices V); k_cands has already
+// counted this win in losses[p].
+__device__ __forceinline__ void winner_features(const Dev& D, const RoundArgs& R, uint32_t p, uint32_t t, uint4 V,
+                                                unsigned long long key, uint32_t better2, uint32_t any2,
+                                                uint32_t rivals, float* f) {
+  const float4 q = D.pts[p];
+  const float depth = vote_score(D.pts, V, q, 0);
+  const uint32_t lost = D.losses[p] ? D.losses[p] - 1u : 0u;
+  const float priority = float(uint32_t(key)) * 2.3283064e-10f;  // hash / 2^32
+  mlp::features(D.pts[V.x], D.pts[V.y], D.pts[V.z], D.pts[V.w], q, depth, lost, R.round, priority, better2, any2,
+                rivals, f);
+}
+
+// Learned scheduler, after k_cands: a vote winner that passes the plain
+// pre-claim filter but finds a better winner's pre-claim in its second ring
+// often loses its cavity to that winner after a full (wasted) search -- but
+// not always: skipping all of them saves a third of the searches and adds
+// rounds.  The fused tensor-core MLP scores the winners (32 per warp,
+// consecutive in the start list) with the predicted probability that they
+// insert this round; those of the second-ring case predicted below
+// deep_threshold wait for the next round (k_bfs skips them).
+__global__ void __launch_bounds__(128) k_sched(Dev D) {
+  const RoundArgs R = load_round(D);
+  if (!R.live) return;
+  constexpr int RS = mlp::kRowStride;
+  __shared__ __align__(16) mlp::Smem S;
+  __shared__ __align__(16) uint32_t rows[4][32 * RS];
+  __shared__ float outs[4][32];
+  __shared__ uint32_t sp[kOrderBuckets + 2];
+  mlp::load_image(S, D.mlp);
+  load_start_prefix(D, sp);
+  const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t nstart = sp[kOrderBuckets + 1];
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + w) * 32; base < nstart; base += warps * 32) {
+    const uint32_t i = base + lane;
+    const bool valid = i < nstart;
+    uint32_t p = 0;
+    bool blocked = false;
+    float f[mlp::kIn];
+#pragma unroll
+    for (int k = 0; k < mlp::kIn; ++k) f[k] = 0.f;
+    bool lost1 = false;
+    if (valid) {
+      p = start_at(D, sp, i);
+      const uint32_t t = D.loc[p];
+      const unsigned long long key = make_key(D, R, p);
+      uint32_t better2, any2, rivals;
+      filter_state(D, R, t, key, lost1, better2, any2, rivals);
+      blocked = !lost1 && better2 > 0;
+      if (blocked) winner_features(D, R, p, t, D.T[t].v, key, better2, any2, rivals, f);
+    }    // the warp scores only if one of its winners needs a decision
+    if (__any_sync(0xFFFFFFFFu, blocked)) {
+      mlp::stage_row(rows[w] + lane * RS, f);
+      __syncwarp();
+      mlp::score32(S, rows[w], outs[w]);
+    }
+    if (valid) {
+      bool defer = lost1 && D.prefilter;  // the plain filter's decision, taken here for k_bfs
+      if (blocked) {
+        float sc = outs[w][lane];
+        sc = (sc == sc) ? fminf(fmaxf(sc, -20.f), 20.f) : -20.f;
+        defer = 1.f / (1.f + __expf(-sc)) < D.deep_threshold;
+      }
+      D.defer[p] = defer ? 1 : 0;
+    }
+    __syncwarp();
+  }
+}
+
+// Scheduler log, after k_cands: features of 1 in 2^log_shift of the winners
+// the learned scheduler decides on (they pass the plain filter and a better
+// winner pre-claimed part of their second ring); label 0 here, set to 1 by
+// k_write when the winner inserts this round.
+__global__ void k_log_features(Dev D) {
+  const RoundArgs R = load_round(D);
+  if (!R.live) return;
+  __shared__ uint32_t sp[kOrderBuckets + 2];
+  load_start_prefix(D, sp);
+  const uint32_t nstart = sp[kOrderBuckets + 1];
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nstart; s += gridDim.x * blockDim.x) {
+    const uint32_t p = start_at(D, sp, s);
+    D.log_pslot[p] = NONE;
+    if ((mix32(p ^ (R.round * 0x27D4EB2Fu)) & ((1u << D.log_shift) - 1u)) != 0u) continue;
+    const uint32_t t = D.loc[p];
+    const unsigned long long key = make_key(D, R, p);
+    bool lost1;
+    uint32_t better2, any2, rivals;
+    filter_state(D, R, t, key, lost1, better2, any2, rivals);
+    if (lost1 || better2 == 0) continue;
+    const uint32_t slot = atomicAdd(&D.st->log_used, 1u);
+    if (slot >= D.log_cap) continue;
+    D.log_pslot[p] = slot;
+    D.log_y[slot] = 0;
+    float f[mlp::kIn];
+    winner_features(D, R, p, t, D.T[t].v, key, better2, any2, rivals, f);
+#pragma unroll
+    for (int k = 0; k < mlp::kIn; ++k) D.log_x[size_t(slot) * mlp::kIn + k] = f[k];
+  }
+}
+
+
 // Candidates: the vote winner of each tet.  Points whose cavity outgrew the
 // warp scratch in an earlier round go to the huge-cavity path.
 __global__ void k_cands(Dev D) {
@@ -899,7 +953,7 @@ __global__ void k_cands(Dev D) {
       p = R.active[i];
       const uint8_t tier = D.bigflag[p];
       const uint32_t t = D.loc[p];
-      if (!(tier & kDup) && t < D.cap && uint32_t(D.vote[t]) == ~p) {
+      if (!(tier & kDup) && t < D.cap && uint32_t(D.C[t].vote) == ~p) {
         if (D.losses && D.losses[p] < 255u) D.losses[p] += 1u;
         if (tier == 2) {
           uint32_t b = atomicAdd(&D.ctr->huge_used, 1u);
@@ -908,13 +962,12 @@ __global__ void k_cands(Dev D) {
           start = true;
           D.st1[p] = 0;
           D.st2[p] = 0;
-          // the learned scheduler pre-claims in k_sched, with its own radius
-          if (D.prefilter && D.vote_mode != 1) pre_claim(D, t, make_key(D, R, p), false);
+          if (D.prefilter) pre_claim(D, t, make_key(D, R, p), false);
         }
       }
     }
     warp_append(&D.ctr->big_used, start);  // total count
-    const uint32_t b = (start && D.order_on) ? (mix32(p ^ (R.round * 0x9E3779B9u)) >> 28) : 0u;
+    const uint32_t b = (start && D.exp_order) ? (mix32(p ^ (R.round * 0x9E3779B9u)) >> 28) : 0u;
     const unsigned grp = __match_any_sync(0xFFFFFFFFu, start ? b : 0xFFFFFFFFu);
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t leader = uint32_t(__ffs(grp) - 1);
@@ -942,9 +995,6 @@ __global__ void k_cands(Dev D) {
 constexpr uint32_t kBfsLanes = 16;
 constexpr uint32_t kWarpGroups = 32 / kBfsLanes;
 constexpr uint32_t kBfsShared = 64;  // queue entries (tet + neighbour words) per group in shared memory
-// Learned scheduler label: a cavity of more tets than a two-ring pre-claim
-// (17) covers is "large".
-constexpr uint32_t kLargeCavity = 17;
 
 // Loads issued as written (volatile asm is neither sunk into the branch that
 // uses the value nor merged with later loads), so that a pass of the cavity
@@ -976,14 +1026,18 @@ __global__ void __launch_bounds__(128, 8) k_bfs(Dev D) {
   uint4* sn = sn_all[threadIdx.x / kBfsLanes];
   uint32_t* cav = D.wscratch + size_t(gid) * BIG_CAP;
   __shared__ uint32_t sp[kOrderBuckets + 2];
+  __shared__ unsigned long long block_searches;
+  if (threadIdx.x == 0) block_searches = 0;
   load_start_prefix(D, sp);
   const uint32_t nstart = sp[kOrderBuckets + 1];
+  unsigned long long searches = 0;
   // Work is taken dynamically, kChunk x kWarpGroups consecutive starts per
   // warp: cavities differ in size by orders of magnitude, and a static
   // grid-stride split leaves warps idle behind the slowest ones.
-  for (uint32_t chunk0 = warp_next(&D.ctr->work[0], kWarpGroups * kChunk); chunk0 < nstart;
-       chunk0 = warp_next(&D.ctr->work[0], kWarpGroups * kChunk))
-  for (uint32_t base = chunk0; base < min(chunk0 + kWarpGroups * kChunk, nstart); base += kWarpGroups) {
+  const uint32_t bchunk = kWarpGroups * D.exp_bchunk;
+  for (uint32_t chunk0 = warp_next(&D.ctr->work[0], bchunk); chunk0 < nstart;
+       chunk0 = warp_next(&D.ctr->work[0], bchunk))
+  for (uint32_t base = chunk0; base < min(chunk0 + bchunk, nstart); base += kWarpGroups) {
     const uint32_t si = base + lane / kBfsLanes;
     bool active = si < nstart;
     uint32_t p = 0, t0 = 0;
@@ -998,22 +1052,24 @@ __global__ void __launch_bounds__(128, 8) k_bfs(Dev D) {
       pq = D.pts[p];
     }
     int pre_lost = 0;
-    if (active && D.prefilter) {
-      const uint32_t nk = (D.ring2 && D.ring2[p]) ? 17u : 5u;
-      for (uint32_t k = gl; k < nk; k += kBfsLanes) {
-        const uint32_t t = k < 5 ? (k == 0 ? t0 : pre_claim_tet(D, t0, 4 * (k - 1) + 1)) : pre_claim_tet(D, t0, k);
-        if (t != NONE && __ldcg(&D.pre[t]) != key) pre_lost = 1;
+    if (active && D.prefilter && !D.defer) {
+      // the winner's own pre-claims (t0 and its face neighbours) must all hold
+      for (uint32_t k = gl; k < 5; k += kBfsLanes) {
+        const uint32_t t = pre_claim_tet(D, t0, k == 0 ? 0u : 4u * (k - 1u) + 1u);
+        if (t != NONE && __ldcg(&D.C[t].pre) != key) pre_lost = 1;
       }
     }
+    // the learned scheduler deferred this winner to the next round
+    if (active && gl == 0 && D.defer && D.defer[p]) pre_lost = 1;
     // warp collectives first, outside any short-circuit: every lane must reach them
     const uint32_t g_pre = (__ballot_sync(FULL, pre_lost) >> shift) & GM;
     const bool searched = active && !g_pre;
     int claim_lost = 0;
     if (searched && gl == 0) {
-      const unsigned long long old = atomicMin(&D.ccav[t0], key);
+      const unsigned long long old = atomicMin(&D.C[t0].cav, key);
       claim_lost = old < key;
       sq[0] = t0;
-      sn[0] = D.tn[t0];
+      sn[0] = D.T[t0].n;
     }
     const int g_claim = __shfl_sync(FULL, claim_lost, shift);
     bool lost = !searched || g_claim;
@@ -1031,17 +1087,17 @@ __global__ void __launch_bounds__(128, 8) k_bfs(Dev D) {
         // the neighbour word comes from the queue (loaded when the tet was
         // added), or from global memory for entries beyond the shared part
         const uint32_t nb = idx < kBfsShared ? comp(sn[idx], int(f))
-                                             : reinterpret_cast<const uint32_t*>(D.tn + cav[idx])[f];
+                                             : reinterpret_cast<const uint32_t*>(&D.T[cav[idx]].n)[f];
         if (nb != NONE) {
           nt = nb >> 2;
           if (nt >= D.cap) {
             my_guard = true;
           } else {
             // one round trip: claim, memo, vertices and neighbours together
-            const unsigned long long cc = ld_cg_u64(&D.ccav[nt]);
-            const unsigned long long cr = ld_cg_u64(&D.cring[nt]);
-            const uint4 W = ld_nc_u4(D.tv + nt);
-            nn = ld_nc_u4(D.tn + nt);
+            const unsigned long long cc = ld_cg_u64(&D.C[nt].cav);
+            const unsigned long long cr = ld_cg_u64(&D.C[nt].ring);
+            const uint4 W = ld_nc_u4(&D.T[nt].v);
+            nn = ld_nc_u4(&D.T[nt].n);
             if (cc != key && cr != key) {
               if (W.x >= D.nv || W.y >= D.nv || W.z >= D.nv || W.w >= D.nv) {
                 my_guard = true;
@@ -1049,11 +1105,11 @@ __global__ void __launch_bounds__(128, 8) k_bfs(Dev D) {
                 const int sg = o4d_sos_f(D.pts[W.x], D.pts[W.y], D.pts[W.z], D.pts[W.w], pq, W.x, W.y, W.z, W.w, p,
                                          D.sos, &D.ctr->err);
                 if (sg < 0) {
-                  const unsigned long long old = atomicMin(&D.ccav[nt], key);
+                  const unsigned long long old = atomicMin(&D.C[nt].cav, key);
                   if (old < key) my_lost = true;
                   else if (old != key) add = true;
                 } else {
-                  D.cring[nt] = key;  // memo for this candidate only
+                  D.C[nt].ring = key;  // memo for this candidate only
                 }
               }
             }
@@ -1089,33 +1145,47 @@ __global__ void __launch_bounds__(128, 8) k_bfs(Dev D) {
       }
       __syncwarp();
     }
-    if (searched && gl == 0) atomicAdd(&D.ctr->n_expanded, 1ull);
-    // scheduler log: is the cavity large (more tets than a two-ring
-    // pre-claim covers)?  Known when the search completed, or once it got
-    // that large before losing.
-    if (D.log_slot && active && gl == 0) {
-      const uint32_t slot = D.log_slot[si];
-      const bool big = overflow || K > kLargeCavity;
-      if (slot != NONE && searched && (big || !lost)) D.log_y[slot] = big ? 1 : 0;
-    }
+    if (searched && gl == 0) ++searches;
     // Partial claims carry this round's key: the huge path takes it next round.
     if (searched && overflow && gl == 0) D.bigflag[p] = kPending | 2;
     bool ok = searched && !lost && !overflow;
-    uint32_t off = 0;
-    if (ok && gl == 0) off = atomicAdd(&D.ctr->pool_used, K);
-    off = __shfl_sync(FULL, off, shift);
+    // One reservation for the warp's completed cavities (pool entries and
+    // candidate slots are shared counters of the whole grid).
+    const uint32_t kk = ok ? K : 0u;
+    const uint32_t kk_lo = __shfl_sync(FULL, kk, 0), kk_hi = __shfl_sync(FULL, kk, kBfsLanes % 32);
+    const uint32_t n_ok = (kk_lo ? 1u : 0u) + (kWarpGroups > 1 && kk_hi ? 1u : 0u);
+    uint32_t off = 0, ci = 0;
+    if (lane == 0 && n_ok) {
+      off = atomicAdd(&D.ctr->pool_used, kk_lo + (kWarpGroups > 1 ? kk_hi : 0u));
+      ci = atomicAdd(&D.ctr->n_cand, n_ok);
+    }
+    off = __shfl_sync(FULL, off, 0);
+    ci = __shfl_sync(FULL, ci, 0);
+    if (shift) {  // the second group follows the first one's entries
+      off += kk_lo;
+      ci += kk_lo ? 1u : 0u;
+    }
     ok = ok && off + K <= D.pool_cap;  // pool full: retry next round
     if (ok) {
       for (uint32_t k = gl; k < K; k += kBfsLanes) D.pool[off + k] = k < kBfsShared ? sq[k] : cav[k];
       if (gl == 0) {
-        const uint32_t ci = atomicAdd(&D.ctr->n_cand, 1u);
         D.cand[ci] = p;
         D.cand_off[ci] = off;
         D.cand_len[ci] = K;
       }
+    } else if (kk && gl == 0) {
+      // a reserved candidate slot whose cavity did not fit the pool: it holds
+      // no cavity, and k_resolve rejects it
+      D.cand[ci] = p;
+      D.cand_off[ci] = 0;
+      D.cand_len[ci] = 0;
     }
     __syncwarp();
   }
+  // per-block statistics, one atomic per block
+  if (searches) atomicAdd(&block_searches, searches);
+  __syncthreads();
+  if (threadIdx.x == 0 && block_searches) atomicAdd(&D.ctr->n_expanded, block_searches);
 }
 
 // Global cavity slot bi of the huge path (HUGE_CAP tets each).
@@ -1146,7 +1216,7 @@ __global__ void __launch_bounds__(256) k_expand_big(Dev D) {
   if (tid == 0) {
     D.st1[p] = 0;
     D.st2[p] = 0;
-    const unsigned long long old = t0 < D.cap ? atomicMin(&D.ccav[t0], key) : 0ull;
+    const unsigned long long old = t0 < D.cap ? atomicMin(&D.C[t0].cav, key) : 0ull;
     sLost = old < key ? 1u : 0u;
     sOver = 0u;
     sGuard = t0 < D.cap ? 0u : 1u;
@@ -1164,20 +1234,20 @@ __global__ void __launch_bounds__(256) k_expand_big(Dev D) {
     const uint32_t idx = head + tid / 4u, f = tid & 3u;
     if (idx < K) {
       const uint32_t c = cav[idx];
-      const uint32_t nb = reinterpret_cast<const uint32_t*>(D.tn + c)[f];
+      const uint32_t nb = reinterpret_cast<const uint32_t*>(&D.T[c].n)[f];
       if (nb != NONE) {
         const uint32_t nt = nb >> 2;
         if (nt >= D.cap) {
           sGuard = 1u;
-        } else if (__ldcg(&D.ccav[nt]) != key && __ldcg(&D.cring[nt]) != key) {
-          const uint4 W = D.tv[nt];
+        } else if (__ldcg(&D.C[nt].cav) != key && __ldcg(&D.C[nt].ring) != key) {
+          const uint4 W = D.T[nt].v;
           if (W.x >= D.nv || W.y >= D.nv || W.z >= D.nv || W.w >= D.nv) {
             sGuard = 1u;
           } else {
             const int sg = o4d_sos_f(D.pts[W.x], D.pts[W.y], D.pts[W.z], D.pts[W.w], pq, W.x, W.y, W.z, W.w, p,
                                      D.sos, &D.ctr->err);
             if (sg < 0) {
-              const unsigned long long old = atomicMin(&D.ccav[nt], key);
+              const unsigned long long old = atomicMin(&D.C[nt].cav, key);
               if (old < key) {
                 sLost = 1u;
               } else if (old != key) {
@@ -1186,7 +1256,7 @@ __global__ void __launch_bounds__(256) k_expand_big(Dev D) {
                 else sOver = 1u;
               }
             } else {
-              D.cring[nt] = key;
+              D.C[nt].ring = key;
             }
           }
         }
@@ -1224,9 +1294,9 @@ __global__ void k_resolve(Dev D) {
     uint32_t K = D.cand_len[ci];
     const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
     unsigned long long key = make_key(D, R, p);
-    bool ok = true;
+    bool ok = K > 0;  // a slot whose cavity did not fit the pool holds none
     for (uint32_t i = lane; i < K; i += 32)
-      if (__ldcg(&D.ccav[cav[i]]) != key) ok = false;
+      if (__ldcg(&D.C[cav[i]].cav) != key) ok = false;
     bool win = __all_sync(0xFFFFFFFFu, ok);
     if (lane == 0) D.st1[p] = win ? 1 : 0;
   }
@@ -1237,7 +1307,7 @@ __device__ __forceinline__ uint32_t slot_of(const Dev& D, const RoundArgs& R, ui
 }
 
 __device__ __forceinline__ bool boundary_face(const Dev& D, uint32_t nb, unsigned long long key) {
-  return nb == NONE || __ldcg(&D.ccav[nb >> 2]) != key;
+  return nb == NONE || __ldcg(&D.C[nb >> 2].cav) != key;
 }
 
 // The edge of face f of tet V opposite corner k (k != f): its two vertex ids,
@@ -1265,88 +1335,138 @@ __global__ void __launch_bounds__(128, 8) k_shared(Dev D) {
   constexpr uint32_t FULL = 0xFFFFFFFFu;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t ncand = __ldcg(&D.ctr->n_cand);
-  for (uint32_t c0 = warp_next(&D.ctr->work[1], kChunk); c0 < ncand; c0 = warp_next(&D.ctr->work[1], kChunk))
-  for (uint32_t ci = c0; ci < min(c0 + kChunk, ncand); ++ci) {
-    const uint32_t p = D.cand[ci];
-    if (!D.st1[p]) {
-      if (lane == 0) D.st2[p] = 0;
-      continue;
-    }
-    const uint32_t K = D.cand_len[ci];
-    const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
-    const unsigned long long key = make_key(D, R, p);
-    // one lane per (cavity tet, face): boundary faces are counted (their
-    // flags kept in a register for cavities of up to 64 tets), faces shared
-    // with a better winner are tested
-    bool bad = false;
-    uint32_t total = 0, bmask = 0;
-    for (uint32_t e0 = 0; e0 < 4 * K; e0 += 32) {
-      const uint32_t e = e0 + lane;
-      bool bnd = false;
-      if (e < 4 * K) {
-        const uint32_t c = cav[e >> 2];
-        const int f = int(e & 3u);
-        const uint32_t nb = reinterpret_cast<const uint32_t*>(D.tn + c)[f];
-        const unsigned long long cc = nb == NONE ? 0ull : __ldcg(&D.ccav[nb >> 2]);
-        bnd = nb == NONE || cc != key;
-        if (bnd && nb != NONE && !bad && cc < key && this_round(R, cc)) {
-          const uint32_t q = key_owner(R, cc);
-          if (q < D.nv && D.st1[q]) {
-            // the new tet on face f: p replaces vertex f
-            const uint4 V = D.tv[c];
-            const uint32_t w0 = f == 0 ? p : V.x, w1 = f == 1 ? p : V.y, w2 = f == 2 ? p : V.z, w3 = f == 3 ? p : V.w;
-            if (o4d_sos_f(D.pts[w0], D.pts[w1], D.pts[w2], D.pts[w3], D.pts[q], w0, w1, w2, w3, q, D.sos,
-                          &D.ctr->err) < 0)
-              bad = true;
+  for (uint32_t c0 = warp_next(&D.ctr->work[1], kChunk); c0 < ncand; c0 = warp_next(&D.ctr->work[1], kChunk)) {
+    // Phase 1, per winner of the chunk: the shared-face test and the count of
+    // boundary faces.  Phase 2: one allocation for the whole chunk (the slot
+    // and list counters are shared by every warp of the grid).  Phase 3: the
+    // slots of each winner's boundary faces.
+    uint32_t need_fresh[kChunk], need_total[kChunk], bmask[kChunk];
+    bool keep[kChunk], inpl[kChunk];
+#pragma unroll
+    for (uint32_t j = 0; j < kChunk; ++j) {
+      const uint32_t ci = c0 + j;
+      keep[j] = false;
+      inpl[j] = false;
+      need_fresh[j] = need_total[j] = bmask[j] = 0;
+      if (ci >= ncand) continue;
+      const uint32_t p = D.cand[ci];
+      if (!D.st1[p]) {
+        if (lane == 0) D.st2[p] = 0;
+        continue;
+      }
+      const uint32_t K = D.cand_len[ci];
+      const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
+      const unsigned long long key = make_key(D, R, p);
+      // one lane per (cavity tet, face): boundary faces are counted (their
+      // flags kept in a register for cavities of up to 64 tets), faces shared
+      // with a better winner are tested
+      bool bad = false;
+      uint32_t total = 0, bm = 0;
+      for (uint32_t e0 = 0; e0 < 4 * K; e0 += 32) {
+        const uint32_t e = e0 + lane;
+        bool bnd = false;
+        if (e < 4 * K) {
+          const uint32_t c = cav[e >> 2];
+          const int f = int(e & 3u);
+          const uint32_t nb = reinterpret_cast<const uint32_t*>(&D.T[c].n)[f];
+          const unsigned long long cc = nb == NONE ? 0ull : __ldcg(&D.C[nb >> 2].cav);
+          bnd = nb == NONE || cc != key;
+          if (bnd && nb != NONE && !bad && cc < key && this_round(R, cc)) {
+            const uint32_t q = key_owner(R, cc);
+            if (q < D.nv && D.st1[q]) {
+              // the new tet on face f: p replaces vertex f
+              const uint4 V = D.T[c].v;
+              const uint32_t w0 = f == 0 ? p : V.x, w1 = f == 1 ? p : V.y, w2 = f == 2 ? p : V.z,
+                             w3 = f == 3 ? p : V.w;
+              if (o4d_sos_f(D.pts[w0], D.pts[w1], D.pts[w2], D.pts[w3], D.pts[q], w0, w1, w2, w3, q, D.sos,
+                            &D.ctr->err) < 0)
+                bad = true;
+            }
           }
         }
+        const uint32_t ball = __ballot_sync(FULL, bnd);
+        total += __popc(ball);
+        if (e0 < 256 && bnd) bm |= 1u << (e0 >> 5);
       }
-      const uint32_t ball = __ballot_sync(FULL, bnd);
-      total += __popc(ball);
-      if (e0 < 256 && bnd) bmask |= 1u << (e0 >> 5);
-    }
-    if (__any_sync(FULL, bad)) {
-      if (lane == 0) D.st2[p] = 0;
-      continue;
-    }
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(&D.ctr->alloc_used, total);
-    base = __shfl_sync(FULL, base, 0);
-    const uint32_t last = base + total;
-    if (last > R.n_freed_prev && R.tet_top + (last - R.n_freed_prev) > D.cap) {
-      if (lane == 0) {
-        atomicOr(&D.ctr->err, kErrCapacity);
-        D.st2[p] = 0;
+      if (__any_sync(FULL, bad)) {
+        if (lane == 0) D.st2[p] = 0;
+        continue;
       }
-      continue;
+      // A small star goes into the cavity's own slots (boundary face r < K
+      // takes the slot of cavity tet r), plus fresh slots for the faces
+      // beyond K: tets that are neighbours in space stay neighbours in memory.
+      // Larger stars take recycled / fresh slots for every face.
+      inpl[j] = D.inplace && total <= kInPlaceFaces && !(D.cand_off[ci] & 0x80000000u);
+      keep[j] = true;
+      need_total[j] = total;
+      need_fresh[j] = total - (inpl[j] ? min(K, total) : 0u);
+      bmask[j] = bm;
     }
-    // slots in (tet, face) order; inner faces get NONE
-    uint32_t run = 0;
-    for (uint32_t e0 = 0; e0 < 4 * K; e0 += 32) {
-      const uint32_t e = e0 + lane;
-      bool bnd = false;
-      uint32_t c = 0;
-      int f = 0;
-      if (e < 4 * K) {
-        c = cav[e >> 2];
-        f = int(e & 3u);
-        if (4 * K <= 256) {
-          bnd = (bmask >> (e0 >> 5)) & 1u;
-        } else {
-          const uint32_t nb = reinterpret_cast<const uint32_t*>(D.tn + c)[f];
-          bnd = boundary_face(D, nb, key);
-        }
-      }
-      const uint32_t ball = __ballot_sync(FULL, bnd);
-      const uint32_t v = base + run + __popc(ball & ((1u << lane) - 1u));
-      if (e < 4 * K) reinterpret_cast<uint32_t*>(D.nslot + c)[f] = bnd ? slot_of(D, R, v) : NONE;
-      if (bnd) D.bface[v] = (c << 2) | uint32_t(f);
-      run += __popc(ball);
+    uint32_t sum_fresh = 0, sum_total = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < kChunk; ++j) {
+      sum_fresh += need_fresh[j];
+      sum_total += need_total[j];
     }
+    if (sum_total == 0) continue;  // warp-uniform
+    uint32_t base = 0, bfo = 0;
     if (lane == 0) {
-      D.cand_base[ci] = base;
-      D.cand_nf[ci] = total;
-      D.st2[p] = 1;
+      base = atomicAdd(&D.ctr->alloc_used, sum_fresh);
+      bfo = atomicAdd(&D.ctr->bface_used, sum_total);
+    }
+    base = __shfl_sync(FULL, base, 0);
+    bfo = __shfl_sync(FULL, bfo, 0);
+#pragma unroll
+    for (uint32_t j = 0; j < kChunk; ++j) {
+      const uint32_t mybase = base, mybfo = bfo;
+      base += need_fresh[j];
+      bfo += need_total[j];
+      if (!keep[j]) continue;
+      const uint32_t ci = c0 + j;
+      const uint32_t p = D.cand[ci];
+      const uint32_t K = D.cand_len[ci];
+      const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
+      const unsigned long long key = make_key(D, R, p);
+      const uint32_t total = need_total[j], fresh = need_fresh[j];
+      const uint32_t reuse = total - fresh;
+      const uint32_t last = mybase + fresh;
+      if ((last > R.n_freed_prev && R.tet_top + (last - R.n_freed_prev) > D.cap) || mybfo + total > D.cap) {
+        if (lane == 0) {
+          atomicOr(&D.ctr->err, kErrCapacity);
+          D.st2[p] = 0;
+        }
+        continue;
+      }
+      // slots in (tet, face) order; inner faces get NONE
+      uint32_t run = 0;
+      for (uint32_t e0 = 0; e0 < 4 * K; e0 += 32) {
+        const uint32_t e = e0 + lane;
+        bool bnd = false;
+        uint32_t c = 0;
+        int f = 0;
+        if (e < 4 * K) {
+          c = cav[e >> 2];
+          f = int(e & 3u);
+          if (4 * K <= 256) {
+            bnd = (bmask[j] >> (e0 >> 5)) & 1u;
+          } else {
+            const uint32_t nb = reinterpret_cast<const uint32_t*>(&D.T[c].n)[f];
+            bnd = boundary_face(D, nb, key);
+          }
+        }
+        const uint32_t ball = __ballot_sync(FULL, bnd);
+        const uint32_t r = run + __popc(ball & ((1u << lane) - 1u));  // rank of this boundary face
+        if (e < 4 * K)
+          reinterpret_cast<uint32_t*>(D.nslot + c)[f] =
+              !bnd ? NONE : (r < reuse ? cav[r] : slot_of(D, R, mybase + (r - reuse)));
+        if (bnd) D.bface[mybfo + r] = (c << 2) | uint32_t(f);
+        run += __popc(ball);
+      }
+      if (lane == 0) {
+        D.cand_base[ci] = mybfo;
+        D.cand_nf[ci] = total | (inpl[j] ? 0x80000000u : 0u);
+        D.st2[p] = 1;
+      }
     }
   }
 }
@@ -1381,6 +1501,15 @@ __global__ void __launch_bounds__(128, 8) k_write(Dev D) {
   const uint32_t w = threadIdx.x >> 5;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t ncand = __ldcg(&D.ctr->n_cand);
+  __shared__ uint32_t block_inserted;
+  __shared__ unsigned long long block_created;
+  if (threadIdx.x == 0) {
+    block_inserted = 0;
+    block_created = 0;
+  }
+  __syncthreads();
+  uint32_t inserted = 0;
+  unsigned long long created = 0;
   for (uint32_t c0 = warp_next(&D.ctr->work[2], kChunk); c0 < ncand; c0 = warp_next(&D.ctr->work[2], kChunk))
   for (uint32_t ci = c0; ci < min(c0 + kChunk, ncand); ++ci) {
     uint32_t p = D.cand[ci];
@@ -1388,8 +1517,10 @@ __global__ void __launch_bounds__(128, 8) k_write(Dev D) {
     uint32_t K = D.cand_len[ci];
     const uint32_t* cav = cand_cavity(D, D.cand_off[ci]);
     unsigned long long key = make_key(D, R, p);
-    const uint32_t F = D.cand_nf[ci];  // boundary faces, counted by k_shared
-    const uint32_t vbase = D.cand_base[ci];  // their allocation (virtual slot) indices
+    const uint32_t nfw = D.cand_nf[ci];
+    const uint32_t F = nfw & 0x7FFFFFFFu;    // boundary faces, counted by k_shared
+    const bool inplace = (nfw >> 31) != 0u;  // the star takes the cavity's own slots
+    const uint32_t bfo = D.cand_base[ci];    // first entry of its boundary-face list
     unsigned long long* tk = nullptr;
     uint32_t *t0 = nullptr, *t1 = nullptr;
     uint32_t mask = 31;
@@ -1421,11 +1552,11 @@ __global__ void __launch_bounds__(128, 8) k_write(Dev D) {
       }
       __syncwarp();
       for (uint32_t j = lane; j < F; j += 32) {
-        const uint32_t bf = D.bface[vbase + j];
+        const uint32_t bf = D.bface[bfo + j];
         const uint32_t c = bf >> 2;
         const int f = int(bf & 3u);
-        const uint32_t sl = slot_of(D, R, vbase + j);
-        const uint4 V = D.tv[c];
+        const uint32_t sl = reinterpret_cast<const uint32_t*>(D.nslot + c)[f];
+        const uint4 V = D.T[c].v;
         {
           for (int k = 0; k < 4; ++k) {
             if (k == f) continue;
@@ -1447,113 +1578,152 @@ __global__ void __launch_bounds__(128, 8) k_write(Dev D) {
       __syncwarp();
     }
     bool bad = false;
-    // one lane per boundary face (the compact list k_shared wrote): each
-    // becomes one new tet
-    for (uint32_t j = lane; j < F; j += 32) {
-      const uint32_t bf = D.bface[vbase + j];
+    // The new tet of boundary face j (the compact list k_shared wrote): the
+    // cavity tet with the face's opposite vertex replaced by p, linked to the
+    // outer tet (or to another winner's new tet on a shared face) and, across
+    // its three faces through p, to its neighbours in the star.
+    auto build = [&](uint32_t j, uint4& nv, uint4& nn, uint32_t& sl, uint32_t& outer, bool& shared) {
+      const uint32_t bf = D.bface[bfo + j];
       const uint32_t c = bf >> 2;
       const int f = int(bf & 3u);
-      const uint32_t sl = slot_of(D, R, vbase + j);
-      const uint4 V = D.tv[c];
-      {
-        uint32_t outer = reinterpret_cast<const uint32_t*>(D.tn + c)[f];
-        bool shared = false;
-        uint32_t link_out = outer;
-        if (outer != NONE) {
-          uint32_t o = outer >> 2;
-          unsigned long long cc = __ldcg(&D.ccav[o]);
-          if (cc != key && this_round(R, cc)) {
-            uint32_t q = key_owner(R, cc);
-            if (q < D.nv && D.st2[q]) {
-              shared = true;
-              link_out = (comp(D.nslot[o], outer & 3) << 2) | (outer & 3);
-            }
+      sl = reinterpret_cast<const uint32_t*>(D.nslot + c)[f];
+      const uint4 V = D.T[c].v;
+      outer = reinterpret_cast<const uint32_t*>(&D.T[c].n)[f];
+      shared = false;
+      uint32_t link_out = outer;
+      if (outer != NONE) {
+        const uint32_t o = outer >> 2;
+        const unsigned long long cc = __ldcg(&D.C[o].cav);
+        if (cc != key && this_round(R, cc)) {
+          const uint32_t q = key_owner(R, cc);
+          if (q < D.nv && D.st2[q]) {
+            shared = true;
+            link_out = (comp(D.nslot[o], outer & 3) << 2) | (outer & 3);
           }
         }
-        uint4 nv = V;
-        set_comp(nv, f, p);
-        uint4 nn = make_uint4(NONE, NONE, NONE, NONE);
-        set_comp(nn, f, link_out);
-        for (int k = 0; k < 4; ++k) {
-          if (k == f) continue;
-          uint32_t link = NONE;
-          if (use_table) {
-            const uint32_t a = edge_lo(V, f, k), b = edge_hi(V, f, k);
-            const unsigned long long ek = (static_cast<unsigned long long>(a) << 32) | b;
-            const uint32_t mine = (sl << 2) | uint32_t(k);
-            uint32_t h = edge_hash(a, b, mask);
-            for (uint32_t probe = 0; probe <= mask; ++probe) {
-              const unsigned long long kk = tk[h];
-              if (kk == ek) {
-                link = t0[h] == mine ? t1[h] : t0[h];
-                break;
-              }
-              if (kk == ~0ull) break;
-              h = (h + 1) & mask;
+      }
+      nv = V;
+      set_comp(nv, f, p);
+      nn = make_uint4(NONE, NONE, NONE, NONE);
+      set_comp(nn, f, link_out);
+      for (int k = 0; k < 4; ++k) {
+        if (k == f) continue;
+        uint32_t link = NONE;
+        if (use_table) {
+          const uint32_t a = edge_lo(V, f, k), b = edge_hi(V, f, k);
+          const unsigned long long ek = (static_cast<unsigned long long>(a) << 32) | b;
+          const uint32_t mine = (sl << 2) | uint32_t(k);
+          uint32_t h = edge_hash(a, b, mask);
+          for (uint32_t probe = 0; probe <= mask; ++probe) {
+            const unsigned long long kk = tk[h];
+            if (kk == ek) {
+              link = t0[h] == mine ? t1[h] : t0[h];
+              break;
             }
-          } else {
-            uint32_t cur = c;
-            uint4 Vc = V;
-            int kc = k, ms = f;
-            for (int it = 0; it < ROT_LIMIT; ++it) {
-              uint32_t nb = comp(D.tn[cur], kc);
-              if (boundary_face(D, nb, key)) {
-                link = (comp(D.nslot[cur], kc) << 2) | uint32_t(ms);
-                break;
-              }
-              uint32_t nt = nb >> 2;
-              if (nt >= D.cap) break;
-              int entry = int(nb & 3);
-              uint32_t x = comp(Vc, ms);
-              uint4 Wt = D.tv[nt];
-              int kx = -1;
-              for (int q = 0; q < 4; ++q)
-                if (comp(Wt, q) == x) kx = q;
-              if (kx < 0) break;
-              cur = nt;
-              Vc = Wt;
-              kc = kx;
-              ms = entry;
-            }
+            if (kk == ~0ull) break;
+            h = (h + 1) & mask;
           }
-          if (link == NONE) bad = true;
-          set_comp(nn, k, link);
+        } else {
+          uint32_t cur = c;
+          uint4 Vc = V;
+          int kc = k, ms = f;
+          for (int it = 0; it < ROT_LIMIT; ++it) {
+            const uint32_t nb = comp(D.T[cur].n, kc);
+            if (boundary_face(D, nb, key)) {
+              link = (comp(D.nslot[cur], kc) << 2) | uint32_t(ms);
+              break;
+            }
+            const uint32_t nt = nb >> 2;
+            if (nt >= D.cap) break;
+            const int entry = int(nb & 3);
+            const uint32_t x = comp(Vc, ms);
+            const uint4 Wt = D.T[nt].v;
+            int kx = -1;
+            for (int q = 0; q < 4; ++q)
+              if (comp(Wt, q) == x) kx = q;
+            if (kx < 0) break;
+            cur = nt;
+            Vc = Wt;
+            kc = kx;
+            ms = entry;
+          }
         }
-        D.tv[sl] = nv;
-        D.tn[sl] = nn;
-        // Every vertex on the cavity boundary gets a live incident tet, so a
-        // vertex's hint tet is alive whenever it is read (strata activation).
-        for (int q = 0; q < 4; ++q)
-          if (q != f) D.vtet[comp(V, q)] = sl;
-        if (outer != NONE && !shared && (outer >> 2) < D.cap) {
-          uint32_t* wp = reinterpret_cast<uint32_t*>(&D.tn[outer >> 2]) + (outer & 3);
-          *wp = (sl << 2) | uint32_t(f);
-        }
+        if (link == NONE) bad = true;
+        set_comp(nn, k, link);
+      }
+    };
+    auto commit = [&](const uint4& nv, const uint4& nn, uint32_t sl, uint32_t outer, bool shared) {
+      D.T[sl].v = nv;
+      D.T[sl].n = nn;
+      // Every vertex on the cavity boundary gets a live incident tet, so a
+      // vertex's hint tet is alive whenever it is read (strata activation).
+      for (int q = 0; q < 4; ++q)
+        if (comp(nv, q) != p) D.vtet[comp(nv, q)] = sl;
+      if (outer != NONE && !shared && (outer >> 2) < D.cap) {
+        uint32_t* wp = reinterpret_cast<uint32_t*>(&D.T[outer >> 2].n) + (outer & 3);
+        const int f = comp(nv, 0) == p ? 0 : comp(nv, 1) == p ? 1 : comp(nv, 2) == p ? 2 : 3;
+        *wp = (sl << 2) | uint32_t(f);
+      }
+    };
+    if (inplace) {
+      // The star overwrites the cavity's own slots: every lane reads first,
+      // the warp synchronises, then every lane writes (F <= 32: one face each).
+      uint4 nv = make_uint4(0, 0, 0, 0), nn = make_uint4(0, 0, 0, 0);
+      uint32_t sl = 0, outer = NONE;
+      bool shared = false;
+      if (lane < F) build(lane, nv, nn, sl, outer, shared);
+      __syncwarp();
+      if (lane < F) commit(nv, nn, sl, outer, shared);
+    } else {
+      for (uint32_t j = lane; j < F; j += 32) {
+        uint4 nv, nn;
+        uint32_t sl, outer;
+        bool shared;
+        build(j, nv, nn, sl, outer, shared);
+        commit(nv, nn, sl, outer, shared);
       }
     }
     if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) atomicOr(&D.ctr->err, kErrRotate);
     __syncwarp();  // every lane is done reading the cavity before it is retired
-    const uint32_t s0 = slot_of(D, R, vbase);
+    uint32_t s0 = 0;
+    if (lane == 0) {
+      const uint32_t bf0 = D.bface[bfo];
+      s0 = reinterpret_cast<const uint32_t*>(D.nslot + (bf0 >> 2))[bf0 & 3u];
+    }
+    s0 = __shfl_sync(0xFFFFFFFFu, s0, 0);
+    // cavity tets whose slots the star did not take are retired
+    const uint32_t reused = inplace ? min(K, F) : 0u;
     uint32_t fbase = 0;
-    if (lane == 0) fbase = atomicAdd(&D.ctr->n_freed_next, K);
+    if (lane == 0 && K > reused) fbase = atomicAdd(&D.ctr->n_freed_next, K - reused);
     fbase = __shfl_sync(0xFFFFFFFFu, fbase, 0);
-    for (uint32_t i = lane; i < K; i += 32) {
-      uint32_t c = cav[i];
+    for (uint32_t i = reused + lane; i < K; i += 32) {
+      const uint32_t c = cav[i];
       // Points inside c relocate from a new tet on one of c's own faces.
-      uint4 S = D.nslot[c];
-      uint32_t fwd = S.x != NONE ? S.x : S.y != NONE ? S.y : S.z != NONE ? S.z : S.w != NONE ? S.w : s0;
-      D.tv[c] = make_uint4(DEAD, fwd, 0u, 0u);
-      R.freed_next[fbase + i] = c;
+      const uint4 S = D.nslot[c];
+      const uint32_t fwd = S.x != NONE ? S.x : S.y != NONE ? S.y : S.z != NONE ? S.z : S.w != NONE ? S.w : s0;
+      D.T[c].v = make_uint4(DEAD, fwd, 0u, 0u);
+      R.freed_next[fbase + (i - reused)] = c;
     }
     if (lane == 0) {
+      if (D.log_pslot && D.log_pslot[p] != NONE) D.log_y[D.log_pslot[p]] = 1;  // scheduler log: inserted
       D.vtet[p] = s0;
       D.loc[p] |= INS_BIT;
       D.centry[D.vcloud[p]] = s0;
       D.bigflag[p] = 0;
-      atomicAdd(&D.ctr->n_inserted, 1u);
-      atomicAdd(&D.ctr->created, (unsigned long long)F);
+      ++inserted;
+      created += F;
     }
     __syncwarp();
+  }
+  // per-block statistics, one atomic each per block
+  if (inserted) {
+    atomicAdd(&block_inserted, inserted);
+    atomicAdd(&block_created, created);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && block_inserted) {
+    atomicAdd(&D.ctr->n_inserted, block_inserted);
+    atomicAdd(&D.ctr->created, block_created);
   }
 }
 
@@ -1579,13 +1749,25 @@ __global__ void __launch_bounds__(512, 2) k_relocate(Dev D) {
         t = 0;
         L |= INS_BIT;
       }
-      D.vote[t] = 0ull;
-      if (D.tcount) D.tcount[t] = 0u;
+      D.C[t].vote = 0ull;
       if (!(L & INS_BIT)) {
         keep = true;
         if (D.bigflag[p] & kPending) D.bigflag[p] &= uint8_t(~kPending);
-        uint4 V = D.tv[t];
-        if (V.x == DEAD) D.loc[p] = walk_to(D, V.y, p, D.pts[p], steps);
+        const uint4 V = D.T[t].v;
+        uint32_t from = NONE;
+        if (V.x == DEAD) {
+          from = V.y;  // retired: walk from a new tet on one of its faces
+        } else {
+          // retired and overwritten by a star in place: t held a cavity tet
+          // of a winner that inserted (its claim is this round's), and now
+          // holds a tet of that winner's star, which covers the point
+          const unsigned long long cc = __ldcg(&D.C[t].cav);
+          if (this_round(R, cc)) {
+            const uint32_t q = key_owner(R, cc);
+            if (q < D.nv && D.st2[q]) from = t;
+          }
+        }
+        if (from != NONE) D.loc[p] = walk_to(D, from, p, D.pts[p], steps);
       }
     }
     uint32_t slot = warp_append(&D.ctr->n_next, keep);
@@ -1642,6 +1824,7 @@ __device__ void begin_round(const Dev& D) {
   C->n_inserted = 0;
   C->huge_used = 0;
   C->btab_used = 0;
+  C->bface_used = 0;
   C->work[0] = C->work[1] = C->work[2] = C->work[3] = 0;
   for (uint32_t b = 0; b <= kOrderBuckets; ++b) C->sbc[b] = 0;
 }
@@ -1710,7 +1893,7 @@ __global__ void k_predicate_signs(const float* pts, const uint32_t* keys, uint64
 __global__ void k_count(Dev D, uint32_t tet_top, uint32_t* ccount, uint32_t* hullcnt, uint2* hull) {
   for (uint32_t t0 = blockIdx.x * blockDim.x; t0 < tet_top; t0 += gridDim.x * blockDim.x) {
     const uint32_t t = t0 + threadIdx.x;
-    uint4 V = t < tet_top ? D.tv[t] : make_uint4(DEAD, 0, 0, 0);
+    uint4 V = t < tet_top ? D.T[t].v : make_uint4(DEAD, 0, 0, 0);
     const bool live = V.x != DEAD;
     const uint32_t c = live ? D.vcloud[V.x] : 0xFFFFFFFFu;
     // one atomic per (warp, cloud) group
@@ -1718,7 +1901,7 @@ __global__ void k_count(Dev D, uint32_t tet_top, uint32_t* ccount, uint32_t* hul
     const int lane = threadIdx.x & 31;
     if (live && lane == __ffs(grp) - 1) atomicAdd(&ccount[c], __popc(grp));
     if (!live) continue;
-    uint4 N = D.tn[t];
+    uint4 N = D.T[t].n;
     for (int f = 0; f < 4; ++f) {
       if (comp(N, f) == NONE) {
         uint32_t h = atomicAdd(&hullcnt[c], 1u);
@@ -1732,7 +1915,7 @@ __global__ void k_count(Dev D, uint32_t tet_top, uint32_t* ccount, uint32_t* hul
 __global__ void k_number(Dev D, uint32_t tet_top, uint32_t* cfill, uint32_t* newid) {
   for (uint32_t t0 = blockIdx.x * blockDim.x; t0 < tet_top; t0 += gridDim.x * blockDim.x) {
     const uint32_t t = t0 + threadIdx.x;
-    uint4 V = t < tet_top ? D.tv[t] : make_uint4(DEAD, 0, 0, 0);
+    uint4 V = t < tet_top ? D.T[t].v : make_uint4(DEAD, 0, 0, 0);
     const bool live = V.x != DEAD;
     const uint32_t c = live ? D.vcloud[V.x] : 0xFFFFFFFFu;
     const unsigned grp = __match_any_sync(0xFFFFFFFFu, c);
@@ -1748,11 +1931,11 @@ __global__ void k_number(Dev D, uint32_t tet_top, uint32_t* cfill, uint32_t* new
 __global__ void k_emit(Dev D, uint32_t tet_top, const uint32_t* newid, const uint64_t* coff, uint32_t* out_t,
                        uint32_t* out_a) {
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < tet_top; t += gridDim.x * blockDim.x) {
-    uint4 V = D.tv[t];
+    uint4 V = D.T[t].v;
     if (V.x == DEAD) continue;
     uint32_t c = D.vcloud[V.x];
     uint64_t row = coff[c] + newid[t];
-    uint4 N = D.tn[t];
+    uint4 N = D.T[t].n;
     uint4 ov = make_uint4(D.sos[V.x], D.sos[V.y], D.sos[V.z], D.sos[V.w]);
     uint4 oa;
     for (int f = 0; f < 4; ++f) {
@@ -1784,7 +1967,7 @@ __global__ void k_infinity(Dev D, const CloudInfo* ci, uint32_t nc, const uint32
   uint32_t base = ccount[c];
   for (int j = 0; j < 4; ++j) {
     uint2 h = hull[4 * c + j];
-    uint4 V = D.tv[h.x];
+    uint4 V = D.T[h.x].v;
     uint32_t w[4] = {D.sos[V.x], D.sos[V.y], D.sos[V.z], D.sos[V.w]};
     w[h.y] = inf;
     int a = -1, b = -1;
@@ -1876,9 +2059,10 @@ struct Workspace {
   DBuf<float4> pts;
   DBuf<uint32_t> sos, vcloud, vtet, loc;
   DBuf<uint8_t> bigflag;
-  DBuf<uint4> tv, tn, nslot;
+  DBuf<Tet> T;
+  DBuf<Claim> C;
+  DBuf<uint4> nslot;
   DBuf<uint32_t> bface;
-  DBuf<unsigned long long> ccav, cring, vote, pre;
   DBuf<uint32_t> centry, active, active_next, cand, cand_off, cand_len, cand_base, cand_nf, pool, big, freed_a, freed_b;
   DBuf<uint8_t> st1, st2;
   DBuf<uint32_t> bigcand, starts, wscratch, etab_val;
@@ -1893,9 +2077,9 @@ struct Workspace {
   DBuf<uint64_t> coff;
   DBuf<uint32_t> out_t, out_a, dtab;
   DBuf<uint8_t> dup;
-  DBuf<uint32_t> tcount, log_slot;
+  DBuf<uint32_t> log_pslot;
   DBuf<uint8_t> losses;
-  DBuf<uint8_t> ring2;
+  DBuf<uint8_t> defer;
   std::vector<DBuf<uint32_t>> scan_tmp;
   Counters* h_ctr = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -1966,15 +2150,15 @@ void release_thread_workspace() {
   Workspace& w = *tl_ws;
   w.xyz.release(); w.off.release(); w.ci.release(); w.mn.release(); w.mx.release();
   w.bucket.release(); w.hist.release(); w.tmp.release(); w.pts.release(); w.sos.release();
-  w.vcloud.release(); w.vtet.release(); w.loc.release(); w.bigflag.release(); w.tv.release();
-  w.tn.release(); w.nslot.release(); w.bface.release(); w.ccav.release(); w.cring.release(); w.pre.release(); w.vote.release();
+  w.vcloud.release(); w.vtet.release(); w.loc.release(); w.bigflag.release(); w.T.release(); w.C.release();
+  w.nslot.release(); w.bface.release();
   w.centry.release(); w.active.release(); w.active_next.release(); w.cand.release();
   w.cand_off.release(); w.cand_len.release(); w.cand_base.release(); w.cand_nf.release(); w.st1.release(); w.st2.release(); w.bigcand.release(); w.starts.release(); w.wscratch.release(); w.pool.release(); w.big.release();
   w.freed_a.release(); w.freed_b.release(); w.lvl_off.release(); w.lvl_total.release(); w.state.release(); w.ctr.release();
   w.ccount.release(); w.hullcnt.release(); w.cfill.release(); w.newid.release();
   w.hull.release(); w.coff.release(); w.out_t.release(); w.out_a.release(); w.dtab.release(); w.dup.release();
   w.etab_key.release(); w.etab_val.release(); w.btab_key.release(); w.btab_val.release();
-  w.tcount.release(); w.log_slot.release(); w.losses.release(); w.ring2.release();
+  w.log_pslot.release(); w.losses.release(); w.defer.release();
   for (auto& b : w.scan_tmp) b.release();
   if (w.h_ctr) cudaFreeHost(w.h_ctr);
   if (w.ev0) cudaEventDestroy(w.ev0);
@@ -2139,6 +2323,10 @@ void reserve_stack_once() {
 
 JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t capacity) {
   reserve_stack_once();
+  {
+    int f = getenv("WTET_F32") ? atoi(getenv("WTET_F32")) : 1;
+    cudaMemcpyToSymbol(g_exp_f32, &f, sizeof(int));
+  }
   Workspace& W = ws();
   // The legacy default stream cannot be captured into a graph; the workspace's
   // own (blocking) stream orders with it implicitly.
@@ -2201,10 +2389,10 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   W.cand_nf.reserve(n, "cand");
   W.st1.reserve(nv, "status");
   W.bigcand.reserve(HUGE_SLOTS, "bigcand");
-  const char* ord_env = getenv("WTET_ORDER");
-  const uint32_t order_on = ord_env ? uint32_t(atoi(ord_env) != 0) : 1u;
-  const uint64_t start_rc = order_on ? (n / kOrderBuckets + n / 64 + 1024) : n;
-  const uint64_t start_ovf = order_on ? start_rc * kOrderBuckets : n;
+  // order-bucket regions: the expected n / kOrderBuckets starts per bucket
+  // plus a 25% margin; anything beyond goes to the overflow region
+  const uint64_t start_rc = n / kOrderBuckets + n / 64 + 1024;
+  const uint64_t start_ovf = start_rc * kOrderBuckets;
   W.starts.reserve(start_ovf + n, "starts");
   // one overflow queue per lane group of a k_bfs wave
   W.wscratch.reserve(size_t(wave(k_bfs, 128)) * (128 / kBfsLanes) * BIG_CAP, "cavity queues");
@@ -2228,18 +2416,13 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   W.hull.reserve(4ull * nc, "hull");
   W.coff.reserve(nc + 1, "coff");
   auto reserve_tets = [&](uint64_t cap) {
-    W.tv.reserve(cap, "tv");
-    W.tn.reserve(cap, "tn");
+    W.T.reserve(cap, "tets");
     W.nslot.reserve(cap, "nslot");
     W.bface.reserve(cap, "boundary faces");
-    W.ccav.reserve(cap, "ccav");
-    W.cring.reserve(cap, "cring");
-    W.pre.reserve(cap, "pre");
-    W.vote.reserve(cap, "vote");
+    W.C.reserve(cap, "claims");
     W.freed_a.reserve(cap, "freed");
     W.freed_b.reserve(cap, "freed");
     W.newid.reserve(cap, "newid");
-    if (vmode) W.tcount.reserve(cap, "tcount");
   };
   reserve_tets(cap0);
   uint64_t cap = cap0;
@@ -2250,31 +2433,32 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   ck(cudaMemsetAsync(W.mx.p, 0x00, 3ull * nc * 4, s), "memset");
   ck(cudaMemsetAsync(W.hist.p, 0, (buckets + 1) * 4, s), "memset");
   ck(cudaMemsetAsync(W.ctr.p, 0, sizeof(Counters), s), "memset");
-  ck(cudaMemsetAsync(W.tv.p, 0xFF, cap * sizeof(uint4), s), "memset");
-  ck(cudaMemsetAsync(W.ccav.p, 0xFF, cap * 8, s), "memset");
-  ck(cudaMemsetAsync(W.cring.p, 0xFF, cap * 8, s), "memset");
-  ck(cudaMemsetAsync(W.pre.p, 0xFF, cap * 8, s), "memset");
-  ck(cudaMemsetAsync(W.vote.p, 0, cap * 8, s), "memset");
+  k_init_slots<<<blocks_for(cap, 256, 148 * 16), 256, 0, s>>>(W.T.p, W.C.p, 0, cap);
   if (vmode) {
     W.losses.reserve(nv, "losses");
-    ck(cudaMemsetAsync(W.tcount.p, 0, cap * 4, s), "memset");
     ck(cudaMemsetAsync(W.losses.p, 0, nv, s), "memset");
   }
-  if (vmode == 2) W.log_slot.reserve(n, "log slots");
+  if (vmode == 2) {
+    W.log_pslot.reserve(nv, "log slots");
+    ck(cudaMemsetAsync(W.log_pslot.p, 0xFF, nv * 4, s), "memset");
+  }
   if (vmode == 1) {
-    W.ring2.reserve(nv, "pre-claim radius");
-    ck(cudaMemsetAsync(W.ring2.p, 0, nv, s), "memset");
+    W.defer.reserve(nv, "deferred winners");
+    ck(cudaMemsetAsync(W.defer.p, 0, nv, s), "memset");
   }
 
   Dev D{};
   auto refresh = [&]() {
     D.pts = W.pts.p; D.sos = W.sos.p; D.vcloud = W.vcloud.p; D.vtet = W.vtet.p; D.loc = W.loc.p;
-    D.bigflag = W.bigflag.p; D.tv = W.tv.p; D.tn = W.tn.p; D.ccav = W.ccav.p; D.cring = W.cring.p;
-    D.nslot = W.nslot.p; D.bface = W.bface.p; D.vote = W.vote.p; D.cap = uint32_t(cap); D.nv = uint32_t(nv); D.centry = W.centry.p;
+    D.bigflag = W.bigflag.p; D.T = W.T.p; D.C = W.C.p;
+    D.nslot = W.nslot.p; D.bface = W.bface.p; D.cap = uint32_t(cap); D.nv = uint32_t(nv); D.centry = W.centry.p;
     D.cand = W.cand.p; D.cand_off = W.cand_off.p;
     D.cand_len = W.cand_len.p; D.cand_base = W.cand_base.p; D.cand_nf = W.cand_nf.p; D.st1 = W.st1.p; D.st2 = W.st2.p; D.bigcand = W.bigcand.p;
-    D.starts = W.starts.p; D.wscratch = W.wscratch.p; D.pre = W.pre.p;
-    D.start_rc = uint32_t(start_rc); D.start_ovf = uint32_t(start_ovf); D.order_on = order_on;
+    D.starts = W.starts.p; D.wscratch = W.wscratch.p;
+    D.start_rc = uint32_t(start_rc); D.start_ovf = uint32_t(start_ovf);
+    D.exp_order = getenv("WTET_ORDER") ? uint32_t(atoi(getenv("WTET_ORDER"))) : 1u;
+    D.exp_bchunk = getenv("WTET_BCHUNK") ? uint32_t(atoi(getenv("WTET_BCHUNK"))) : 1u;
+    D.inplace = getenv("WTET_INPLACE") ? uint32_t(atoi(getenv("WTET_INPLACE"))) : 1u;
     D.etab_key = W.etab_key.p; D.etab_val = W.etab_val.p; D.etab_warps = etab_warps;
     D.btab_key = W.btab_key.p; D.btab_val = W.btab_val.p;
     D.prefilter = cfg.candidate_filter == 2 ? 0u : 1u; D.pool = W.pool.p; D.pool_cap = pool_cap; D.big = W.big.p;
@@ -2284,14 +2468,13 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     D.lvl_total = W.lvl_total.p; D.nc = nc;
     D.rule = int(job.cfg.insertion_rule == WTET_RULE_CENTROID ? 1 : 0);
     D.vote_mode = vmode;
-    D.tcount = vmode ? W.tcount.p : nullptr;
     D.losses = vmode ? W.losses.p : nullptr;
     D.mlp = mlp_w;
-    D.ring2 = vmode == 1 ? W.ring2.p : nullptr;
+    D.defer = vmode == 1 ? W.defer.p : nullptr;
     D.deep_threshold = (cfg.deep_threshold ? float(cfg.deep_threshold) : 64.f) / 256.f;
     D.log_x = job.d_log_x;
     D.log_y = job.d_log_y;
-    D.log_slot = vmode == 2 ? W.log_slot.p : nullptr;
+    D.log_pslot = vmode == 2 ? W.log_pslot.p : nullptr;
     D.log_cap = uint32_t(std::min<uint64_t>(job.log_cap, 0xFFFFFFF0ull));
     D.log_shift = std::min<uint32_t>(job.log_shift, 31u);
   };
@@ -2365,46 +2548,72 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   // one full wave of resident blocks: an idle round then costs one short
   // wave per kernel.
   const uint32_t GB = HUGE_SLOTS;  // one block per huge-cavity slot
-  const uint32_t g_act = wave(k_activate, TB), g_tc = wave(k_tcount, TB), g_vote = wave(k_vote, TB);
-  const uint32_t g_cand = wave(k_cands, TB), g_sched = wave(k_sched, 128), g_logf = wave(k_log_features, TB);
-  const uint32_t g_bfs = wave(k_bfs, 128), g_res = wave(k_resolve, 128), g_sh = wave(k_shared, 128);
-  const uint32_t g_wr = wave(k_write, 128), g_rel = wave(k_relocate, TB);
-  const uint64_t kernels_per_round = 10 + (vmode ? 2 : 0);
+  struct Grids {
+    uint32_t act, vote, cand, sched, logf, bfs, res, sh, wr, rel;
+  };
+  const Grids big{wave(k_activate, TB), wave(k_vote, TB),      wave(k_cands, TB),  wave(k_sched, 128),
+                  wave(k_log_features, TB), wave(k_bfs, 128), wave(k_resolve, 128), wave(k_shared, 128),
+                  wave(k_write, 128),  wave(k_relocate, TB)};
+  // Rounds of the first strata have a few thousand points: a full wave of
+  // blocks that exit at once costs more than their work, so those rounds
+  // replay a graph with one block per SM.
+  auto shrink = [](uint32_t g) { return std::min<uint32_t>(g, 148u); };
+  const Grids small{shrink(big.act), shrink(big.vote), shrink(big.cand), shrink(big.sched), shrink(big.logf),
+                    shrink(big.bfs), shrink(big.res),  shrink(big.sh),   shrink(big.wr),    shrink(big.rel)};
+  const uint64_t kernels_per_round = 10 + (vmode ? 1 : 0);
 
   // One round: k_end also starts the next round (k_begin starts the first).
-  auto enqueue_round = [&]() {
-    k_activate<<<g_act, TB, 0, s>>>(D);
-    if (vmode) k_tcount<<<g_tc, TB, 0, s>>>(D);
-    k_vote<<<g_vote, TB, 0, s>>>(D);
-    k_cands<<<g_cand, TB, 0, s>>>(D);
-    if (vmode == 1) k_sched<<<g_sched, 128, 0, s>>>(D);
-    if (vmode == 2) k_log_features<<<g_logf, TB, 0, s>>>(D);
-    k_bfs<<<g_bfs, 128, 0, s>>>(D);
+  auto enqueue_round = [&](const Grids& G) {
+    k_activate<<<G.act, TB, 0, s>>>(D);
+    k_vote<<<G.vote, TB, 0, s>>>(D);
+    k_cands<<<G.cand, TB, 0, s>>>(D);
+    if (vmode == 1) k_sched<<<G.sched, 128, 0, s>>>(D);
+    if (vmode == 2) k_log_features<<<G.logf, TB, 0, s>>>(D);
+    k_bfs<<<G.bfs, 128, 0, s>>>(D);
     k_expand_big<<<GB, 256, 0, s>>>(D);
-    k_resolve<<<g_res, 128, 0, s>>>(D);
-    k_shared<<<g_sh, 128, 0, s>>>(D);
-    k_write<<<g_wr, 128, 0, s>>>(D);
-    k_relocate<<<g_rel, TB, 0, s>>>(D);
+    k_resolve<<<G.res, 128, 0, s>>>(D);
+    k_shared<<<G.sh, 128, 0, s>>>(D);
+    k_write<<<G.wr, 128, 0, s>>>(D);
+    k_relocate<<<G.rel, TB, 0, s>>>(D);
     k_end<<<1, 32, 0, s>>>(D);
   };
   // Rounds per host check (the graph holds this many rounds).
   uint32_t rpg = std::min<uint32_t>(cfg.rounds_per_graph, 64u);
   if (trace) rpg = 1;
-  cudaGraphExec_t gexec = nullptr;
+  cudaGraphExec_t gexec = nullptr, gexec_small = nullptr;
+  auto capture = [&](const Grids& G) {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t e = nullptr;
+    ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+    for (uint32_t r = 0; r < rpg; ++r) enqueue_round(G);
+    ck(cudaStreamEndCapture(s, &g), "end capture");
+    ck(cudaGraphInstantiate(&e, g, 0), "graph instantiate");
+    cudaGraphDestroy(g);
+    return e;
+  };
   auto build_graph = [&]() {
     if (gexec) cudaGraphExecDestroy(gexec);
-    gexec = nullptr;
-    cudaGraph_t g = nullptr;
-    ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
-    for (uint32_t r = 0; r < rpg; ++r) enqueue_round();
-    ck(cudaStreamEndCapture(s, &g), "end capture");
-    ck(cudaGraphInstantiate(&gexec, g, 0), "graph instantiate");
-    cudaGraphDestroy(g);
+    if (gexec_small) cudaGraphExecDestroy(gexec_small);
+    gexec = capture(big);
+    gexec_small = capture(small);
   };
+  auto destroy_graphs = [&]() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (gexec_small) cudaGraphExecDestroy(gexec_small);
+    gexec = gexec_small = nullptr;
+  };
+  // Points the next graph launch may see: the current list and the next two
+  // strata (each stratum about doubles the previous one).
+  auto upcoming = [&](const State& h) {
+    uint64_t u = h.n_active;
+    for (int L = h.next_level, k = 0; L >= 0 && k < 2; --L, ++k) u += lvl_total[L];
+    return u;
+  };
+  constexpr uint64_t kSmallRoundPoints = 32768;
   build_graph();
   k_begin<<<1, 32, 0, s>>>(D);
   launches += 1;
-  State hs{};
+  State hs = S0;
   cudaEvent_t tr0 = nullptr, tr1 = nullptr;  // per-round device time when tracing
   if (trace) {
     ck(cudaEventCreate(&tr0), "event");
@@ -2412,7 +2621,7 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   }
   for (;;) {
     if (trace) ck(cudaEventRecord(tr0, s), "event record");
-    ck(cudaGraphLaunch(gexec, s), "graph launch");
+    ck(cudaGraphLaunch(upcoming(hs) <= kSmallRoundPoints ? gexec_small : gexec, s), "graph launch");
     if (trace) ck(cudaEventRecord(tr1, s), "event record");
     launches += uint64_t(rpg) * kernels_per_round;
     ck(cudaMemcpyAsync(&hs, W.state.p, sizeof(State), cudaMemcpyDeviceToHost, s), "d2h");
@@ -2429,13 +2638,13 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
               hs.last_inserted, (unsigned long long)h.n_big, hs.last_alloc, hs.tet_top, h.err, rms);
     }
     if (hs.stop == 1) {
-      if (gexec) cudaGraphExecDestroy(gexec);
+      destroy_graphs();
       char buf[160];
       snprintf(buf, sizeof buf, "device consistency check failed (flags 0x%x) in round %u", h.err, hs.round);
       throw Error{(h.err & kErrPrec) ? WTET_ERR_PRECISION : WTET_ERR_INTERNAL, buf};
     }
     if (hs.stop == 3) {
-      if (gexec) cudaGraphExecDestroy(gexec);
+      destroy_graphs();
       throw Error{WTET_ERR_NO_CONVERGE, "insertion did not converge within max_insert_iterations"};
     }
     if (hs.stop == 2) {
@@ -2443,26 +2652,14 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
       uint64_t ncap = std::min<uint64_t>(cap * 3 / 2 + 1024, 0x7FFFFFF0ull);
       if (ncap <= cap) throw Error{WTET_ERR_CAPACITY, "tet capacity exhausted"};
       const uint32_t top = hs.tet_top;
-      W.tv.grow_keep(ncap, top, s, "grow tv");
-      ck(cudaMemsetAsync(W.tv.p + top, 0xFF, (ncap - top) * sizeof(uint4), s), "memset");
-      W.tn.grow_keep(ncap, top, s, "grow tn");
+      W.T.grow_keep(ncap, top, s, "grow tets");
+      W.C.grow_keep(ncap, top, s, "grow claims");
+      k_init_slots<<<blocks_for(ncap - top, 256, 148 * 16), 256, 0, s>>>(W.T.p, W.C.p, top, ncap);
       W.nslot.grow_keep(ncap, 0, s, "grow nslot");
       W.bface.grow_keep(ncap, 0, s, "grow boundary faces");
-      W.ccav.grow_keep(ncap, top, s, "grow ccav");
-      ck(cudaMemsetAsync(W.ccav.p + top, 0xFF, (ncap - top) * 8, s), "memset");
-      W.cring.grow_keep(ncap, top, s, "grow cring");
-      ck(cudaMemsetAsync(W.cring.p + top, 0xFF, (ncap - top) * 8, s), "memset");
-      W.pre.grow_keep(ncap, top, s, "grow pre");
-      ck(cudaMemsetAsync(W.pre.p + top, 0xFF, (ncap - top) * 8, s), "memset");
-      W.vote.grow_keep(ncap, top, s, "grow vote");
-      ck(cudaMemsetAsync(W.vote.p + top, 0, (ncap - top) * 8, s), "memset");
       W.freed_a.grow_keep(ncap, ncap > 0 ? W.freed_a.n : 0, s, "grow freed");
       W.freed_b.grow_keep(ncap, W.freed_b.n, s, "grow freed");
       W.newid.grow_keep(ncap, 0, s, "grow newid");
-      if (vmode) {
-        W.tcount.grow_keep(ncap, 0, s, "grow tcount");
-        ck(cudaMemsetAsync(W.tcount.p, 0, ncap * 4, s), "memset");
-      }
       cap = ncap;
       st.capacity_grows += 1;
       refresh();
@@ -2478,7 +2675,7 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     }
     if (hs.done) break;
   }
-  if (gexec) cudaGraphExecDestroy(gexec);
+  destroy_graphs();
   if (tr0) cudaEventDestroy(tr0);
   if (tr1) cudaEventDestroy(tr1);
   const uint32_t tet_top = hs.tet_top;

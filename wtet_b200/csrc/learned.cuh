@@ -1,17 +1,20 @@
 // Learned insertion scheduler: per vote-winner features and the fused BF16
-// MLP that predicts whether the winner's cavity is large (more tets than a
-// two-ring pre-claim covers).
+// MLP that predicts whether a vote winner will insert this round.
 //
 // The reference orders insertions by the circumsphere determinant alone
 // (src/shaders/vote.wgsl:401-494); it has no learned scheduler.  Here every
 // tet still votes for the point deepest in its circumsphere, and each winner
-// pre-claims its tet's neighbourhood; a winner whose neighbourhood overlaps a
-// better one's skips its cavity search this round.  Winners the network (12
-// -> 64 -> 64 -> 64 -> 1, ReLU, BF16 weights and activations, FP32
-// accumulate; trained on the plain method's own logs) predicts to have large
-// cavities pre-claim two rings of neighbours, the rest one.  Only the order
-// changes: every round still inserts an exactly Delaunay-compatible set of
-// points, so the final tet set is the same unique SoS triangulation.
+// pre-claims its tet and face neighbours; a winner whose pre-claims a better
+// one overwrote skips its cavity search this round (the plain method).  A
+// winner that passes but finds a better winner's pre-claim in its second ring
+// of neighbours often loses its cavity later, after a wasted search -- but
+// not always: skipping all of them saves a third of the searches and costs
+// rounds.  The network (12 -> 64 -> 64 -> 64 -> 1, ReLU, BF16 weights and
+// activations, FP32 accumulate; trained on the plain method's own logs)
+// predicts, for those winners, whether they would insert anyway; the ones
+// predicted to fail wait for the next round.  Only the order changes: every
+// round still inserts an exactly Delaunay-compatible set of points, so the
+// final tet set is the same unique SoS triangulation.
 //
 // Inference runs on the tensor cores with warp-level mma.m16n8k16 (BF16 in,
 // FP32 accumulate): each warp scores 32 winners at a time, the activations
@@ -174,15 +177,15 @@ __device__ __forceinline__ float finite_or(float x, float dflt) { return isfinit
 __device__ __forceinline__ float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
 
 // The 12 features of vote winner q in tet (a, b, c, d), all O(1) by construction:
-//  0 |q - circumcenter|^2 / R^2          6 log2(1 + round) / 8
-//  1 log2(insphere depth) / 64           7 log2(Morton-neighbour distance / emax) / 8
-//  2 shortest / longest edge             8 face-neighbour tets holding a rival winner / 4
-//  3 6*sqrt(2)*V / emax^3 (1 = regular)  9 sum over face neighbours of log2(1 + their points) / 32
-//  4 log2(R / emax) / 4                 10 log2(1 + earlier wins of q that did not insert) / 4
-//  5 log2(1 + uninserted points in tet) / 8   11 tet has a super vertex
-__device__ __forceinline__ void features(float4 a, float4 b, float4 c, float4 d, float4 q, float depth, uint32_t count,
-                                         uint32_t losses, uint32_t round, float nbr_dist, uint32_t rivals,
-                                         float crowd, float* f) {
+//  0 |q - circumcenter|^2 / R^2          6 claim priority of q this round (0 = best, 1 = worst)
+//  1 log2(insphere depth) / 64           7 second-ring tets pre-claimed by a better winner / 12
+//  2 6*sqrt(2)*V / emax^3 (1 = regular)  8 face-neighbour tets holding a vote winner / 4
+//  3 log2(R / emax) / 4                  9 share of the second ring's winners that are better
+//  4 second-ring tets pre-claimed by any winner / 12   10 log2(1 + earlier wins of q that did not insert) / 4
+//  5 log2(1 + round) / 8                11 tet has a super vertex
+__device__ __forceinline__ void features(float4 a, float4 b, float4 c, float4 d, float4 q, float depth,
+                                         uint32_t losses, uint32_t round, float priority, uint32_t better2,
+                                         uint32_t any2, uint32_t rivals, float* f) {
   const float abx = b.x - a.x, aby = b.y - a.y, abz = b.z - a.z;
   const float acx = c.x - a.x, acy = c.y - a.y, acz = c.z - a.z;
   const float adx = d.x - a.x, ady = d.y - a.y, adz = d.z - a.z;
@@ -192,7 +195,6 @@ __device__ __forceinline__ void features(float4 a, float4 b, float4 c, float4 d,
   const float lab = abx * abx + aby * aby + abz * abz, lac = acx * acx + acy * acy + acz * acz;
   const float lad = adx * adx + ady * ady + adz * adz, lbc = bcx * bcx + bcy * bcy + bcz * bcz;
   const float lbd = bdx * bdx + bdy * bdy + bdz * bdz, lcd = cdx * cdx + cdy * cdy + cdz * cdz;
-  const float emin2 = fminf(fminf(fminf(lab, lac), fminf(lad, lbc)), fminf(lbd, lcd));
   const float emax2 = fmaxf(fmaxf(fmaxf(lab, lac), fmaxf(lad, lbc)), fmaxf(lbd, lcd));
   const float emax = sqrtf(emax2);
   // cross products for the circumcenter (relative to a)
@@ -211,14 +213,14 @@ __device__ __forceinline__ void features(float4 a, float4 b, float4 c, float4 d,
                    d.x < -50.f || d.x > 200.f;
   f[0] = clampf(finite_or((qx * qx + qy * qy + qz * qz) / R2, 1.f), 0.f, 1.f);
   f[1] = clampf(finite_or(__log2f(depth + 1e-37f), -128.f) * (1.f / 64.f), -2.f, 2.f);
-  f[2] = clampf(finite_or(sqrtf(emin2 / emax2), 0.f), 0.f, 1.f);
-  f[3] = clampf(finite_or(av6 * 1.41421356f / (emax2 * emax), 0.f), 0.f, 1.f);
-  f[4] = clampf(finite_or(0.5f * __log2f(R2 / emax2), 8.f), -8.f, 8.f) * 0.25f;
-  f[5] = __log2f(1.f + float(count)) * 0.125f;
-  f[6] = __log2f(1.f + float(round)) * 0.125f;
-  f[7] = clampf(finite_or(__log2f(nbr_dist / emax), -16.f), -16.f, 16.f) * 0.125f;
+  f[2] = clampf(finite_or(av6 * 1.41421356f / (emax2 * emax), 0.f), 0.f, 1.f);
+  f[3] = clampf(finite_or(0.5f * __log2f(R2 / emax2), 8.f), -8.f, 8.f) * 0.25f;
+  f[4] = float(any2) * (1.f / 12.f);
+  f[5] = __log2f(1.f + float(round)) * 0.125f;
+  f[6] = priority;
+  f[7] = float(better2) * (1.f / 12.f);
   f[8] = float(rivals) * 0.25f;
-  f[9] = crowd * (1.f / 32.f);
+  f[9] = any2 ? float(better2) / float(any2) : 0.f;
   f[10] = __log2f(1.f + float(losses)) * 0.25f;
   f[11] = sup ? 1.f : 0.f;
 }

@@ -2,22 +2,22 @@
 
 Every tet votes for its uninserted point deepest inside its circumsphere (the
 reference's vote, src/shaders/vote.wgsl:401-494).  Each vote winner then
-pre-claims its tet's neighbourhood, and a winner whose neighbourhood overlaps
-a better one's skips its cavity search this round.  Pre-claiming only the ring
-of face neighbours misses the conflicts of large cavities (found later, after
-an expensive wasted search); pre-claiming two rings for everyone blocks small
-cavities that would not have met and costs rounds.  ``Config(vote="learned")``
-lets a small MLP (12 -> 64 -> 64 -> 64 -> 1, ReLU) predict, per winner,
-whether its cavity is large (more tets than a two-ring pre-claim covers), and
-only those winners pre-claim two rings.
-Inference is fused into the kernel that schedules the winners (BF16
-tensor-core mma, FP32 accumulate); the triangulation is unchanged, only the
-order of insertions.
+pre-claims its tet and face neighbours, and a winner whose pre-claims a
+better winner overwrote skips its cavity search this round (the plain
+method).  A winner that passes this filter but finds a better winner's
+pre-claim in its second ring often loses its cavity to that winner after a
+full, wasted search -- but not always, and skipping all of them costs rounds.
+``Config(vote="learned")`` lets a small MLP (12 -> 64 -> 64 -> 64 -> 1, ReLU)
+predict, for those winners, whether they would insert this round anyway; the
+ones predicted to fail wait for the next round.  Inference is fused into the
+kernel that schedules the winners (BF16 tensor-core mma, FP32 accumulate);
+the triangulation is unchanged, only the order of insertions.
 
 Everything here runs on the GPU through libwtet.so:
 
 * ``collect``  -- training records from the plain method's own runs: the
-  features of sampled vote winners and whether each one's cavity is large;
+  features of sampled winners of that second-ring case and whether each
+  one inserted in its round;
 * ``train``    -- the project's forward / backward / Adam kernels;
 * ``loss_grad`` -- one forward + backward pass (checked against a CPU
   restatement in the tests);
@@ -37,14 +37,14 @@ from . import _core
 FEATURES = (
     "circumcenter_distance",   # |q - c|^2 / R^2
     "insphere_depth",          # log2 of the plain vote's circumsphere depth / 64
-    "edge_ratio",              # shortest / longest edge
     "volume_ratio",            # 6 sqrt(2) V / emax^3
     "circumradius_ratio",      # log2(R / emax) / 4
-    "points_in_tet",           # log2(1 + uninserted points in the tet) / 8
+    "second_ring_winners",     # second-ring tets pre-claimed by any winner / 12
     "round",                   # log2(1 + round) / 8
-    "neighbour_distance",      # log2(Morton-neighbour distance / emax) / 8
-    "rival_neighbours",        # face-neighbour tets holding another winner / 4
-    "neighbour_crowding",      # sum over face neighbours of log2(1 + their points) / 32
+    "claim_priority",          # the winner's claim hash this round / 2^32 (0 = best)
+    "better_second_ring",      # second-ring tets pre-claimed by a better winner / 12
+    "rival_neighbours",        # face-neighbour tets holding a vote winner / 4
+    "better_share",            # share of the second ring's winners that are better
     "failed_attempts",         # log2(1 + earlier vote wins without insertion) / 4
     "super_vertex",            # the tet has a super vertex
 )
@@ -125,9 +125,10 @@ def load_default(path: str = DEFAULT_WEIGHTS) -> np.ndarray:
 def collect(clouds, config: _core.Config | None = None, capacity: int | None = None, sample_shift: int = 0):
     """Training records (X (m, 12) float32, y (m,) uint8, stats) from the
     plain method's run on ``clouds`` (list of (N, 3) arrays): features of 1 in
-    2**sample_shift vote winners and whether each one's cavity is large (more
-    than 17 tets; winners whose search stopped before that was known are
-    dropped)."""
+    2**sample_shift of the vote winners the learned scheduler decides on (they
+    pass the plain pre-claim filter and a better winner pre-claimed part of
+    their second ring), and whether each one inserted in its round (1) or not
+    (0)."""
     arrs = [_core._points(c) for c in clouds]
     offsets = np.zeros(len(arrs) + 1, np.uint64)
     offsets[1:] = np.cumsum([a.shape[0] for a in arrs])
@@ -201,7 +202,8 @@ def training_clouds(seeds=(1, 2, 3, *range(11, 31)), size: int = 200_000):
     """The training distribution, from the small plain, degenerate and large
     plain configurations: per seed a 100k uniform cloud, a mixture cloud, a
     thin shell and a unit sphere (``size`` points, halved for the last two),
-    plus exact lattices of 32^3, 48^3 and 64^3 points."""
+    2M-point mixture clouds from four of the seeds, and exact lattices of
+    32^3, 48^3 and 64^3 points."""
     from . import synthetic as syn
 
     for s in seeds:
@@ -209,6 +211,8 @@ def training_clouds(seeds=(1, 2, 3, *range(11, 31)), size: int = 200_000):
         yield [syn.mixture(size, s)]
         yield [syn.sphere_shell(size // 2, s)]
         yield [syn.unit_sphere(size // 2, s)]
+    for s in seeds[3:7]:
+        yield [syn.mixture(2_000_000, s)]
     for k in (32, 48, 64):
         yield [syn.lattice(k)]
 
@@ -233,10 +237,24 @@ def make_default(path: str = DEFAULT_WEIGHTS, epochs: int = 6, sample_shift: int
     s = score(X[va])
     acc = float(((s > 0) == (y[va] > 0.5)).mean())
     base = float(max(y[va].mean(), 1 - y[va].mean()))
+    auc = roc_auc(s, y[va])
     if verbose:
         print(f"records {X.shape[0]} positive {y.mean():.3f} epoch losses {np.round(losses, 4).tolist()} "
-              f"val acc {acc:.4f} (majority {base:.4f})")
-    os.makedirs(os.path.dirname(path), exist_ok=True)
-    np.savez(path, params=params, epoch_loss=losses, val_accuracy=acc, majority=base, records=X.shape[0],
-             positive_rate=float(y.mean()), sample_shift=sample_shift, seed=seed)
+              f"val acc {acc:.4f} (majority {base:.4f}) auc {auc:.3f}")
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    np.savez(path, params=params, epoch_loss=losses, val_accuracy=acc, majority=base, val_auc=auc,
+             records=X.shape[0], positive_rate=float(y.mean()), sample_shift=sample_shift, seed=seed)
     return params
+
+
+def roc_auc(scores, labels) -> float:
+    """Area under the ROC curve of scores for binary labels (rank statistic)."""
+    scores = np.asarray(scores, np.float64)
+    pos = np.asarray(labels) > 0.5
+    order = np.argsort(scores, kind="stable")
+    ranks = np.empty(len(scores))
+    ranks[order] = np.arange(1, len(scores) + 1)
+    npos, nneg = int(pos.sum()), int((~pos).sum())
+    if npos == 0 or nneg == 0:
+        return 0.5
+    return float((ranks[pos].sum() - npos * (npos + 1) / 2) / (npos * nneg))
