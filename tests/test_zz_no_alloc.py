@@ -1,11 +1,18 @@
 """The allocation-free quality check, wtet_check_quality_noalloc.
 
-It exists for callers that must not allocate GPU memory while it runs (stream
-capture in progress, serving loops on an allocator owned by another framework,
-fixed memory budgets), so its scratch is a fixed device array inside
-libwtet.so.  These tests call it through the C ABI and check that two calls in
-a row return exactly what the allocating wtet_check_quality returns, and that
-sizes beyond its fixed scratch are refused.  Collected last on purpose.
+It exists for callers that must not allocate GPU memory while it runs
+(serving loops whose GPU memory belongs to an allocator another framework
+owns, hosts with a memory budget fixed up front), so its scratch is a fixed
+device array inside libwtet.so.  These tests call it through the C ABI and
+check that two calls in a row return exactly what the allocating
+wtet_check_quality returns, and that sizes beyond its fixed scratch are
+refused.
+
+The file name sorts last so that pytest collects it after every other test:
+the array is shared by every call in the process, so running it after the
+rest shows that earlier work leaves nothing in the array that changes its
+result, and a run that stops at the first failure has run everything else
+first.  It also passes alone in a fresh process.
 """
 import ctypes
 
