@@ -71,9 +71,9 @@ typedef struct wtet_config {
   uint32_t candidate_filter;       /* neighbourhood pre-claim before cavity growth: 1 = on (default),
                                       2 = off */
   uint32_t pool_factor;            /* cavity-pool entries per point (default 24, 4..64) */
-  uint32_t deep_threshold;         /* learned scheduler: a winner it decides on waits for the next
-                                      round when its predicted probability of inserting is below
-                                      deep_threshold/256; 0 = default (64, i.e. 1/4) */
+  uint32_t learned_gate;           /* learned scheduler: rounds whose graph may see at most
+                                      learned_gate x 1024 uninserted points take the network's claim
+                                      priority, larger rounds the hashed one; 0 = default (2048) */
   uint32_t initial_capacity;       /* initial tet slots per point, in eighths; 0 = default (72, i.e. 9
                                       per point).  When a round runs out of slots the tet arrays grow
                                       in place by half (stats.capacity_grows counts it); small values
@@ -227,13 +227,14 @@ int wtet_predicate_signs(const float* pts, const uint32_t* keys, uint64_t m, int
 /* ---- Learned insertion scheduler (no counterpart in the reference, which
  * orders insertions by the circumsphere determinant alone,
  * src/shaders/vote.wgsl:401-494).  Every tet votes for its point deepest in
- * its circumsphere; each winner pre-claims its tet and face neighbours, and a
- * winner whose pre-claims a better one overwrote skips its cavity search this
- * round (the plain method).  With vote_mode = WTET_VOTE_LEARNED a 12 -> 64 ->
- * 64 -> 64 -> 1 ReLU MLP scores the winners that pass this filter but find a
- * better winner's pre-claim in their second ring of neighbours: those it
- * predicts not to insert this round wait for the next one instead of
- * searching a cavity they would most likely lose.  Only the order of
+ * its circumsphere; the vote winners then compete for their cavities by claim
+ * keys (the smaller key wins a contested tet), hashed in the plain method.
+ * With vote_mode = WTET_VOTE_LEARNED a 12 -> 64 -> 64 -> 64 -> 1 ReLU MLP,
+ * fused into the kernel that turns votes into winners, predicts each winner's
+ * probability of inserting in this round under hashed keys, and the winners
+ * least likely to insert (crowded neighbourhoods, which set the number of
+ * rounds) get the smallest keys.  It serves the rounds of the first strata
+ * (learned_gate); the bulk rounds keep hashed keys.  Only the order of
  * insertions changes: the output is the same tet set.
  *
  * Parameters are FP32 in one flat array of WTET_MLP_PARAMS values:
@@ -252,10 +253,10 @@ int wtet_learned_has_weights(void);
 
 /* Training data from the plain method's own runs: triangulates the clouds
  * (layout of wtet_delaunay_batched) with the plain scheduler and records, for
- * 1 in 2^sample_shift of the winners the learned scheduler decides on (they
- * pass the pre-claim filter and a better winner pre-claimed part of their
- * second ring), the 12 features (features, capacity x 12) and the label
- * (labels, capacity): 1 if the winner inserted in its round, 0 if not.
+ * 1 in 2^sample_shift of the vote winners in the rounds the learned scheduler
+ * serves (cfg->learned_gate), the 12 features (features, capacity x 12) and
+ * the label (labels, capacity): 1 if the winner inserted in its round, 0 if
+ * not.
  * *count receives the records written (at most capacity).  The triangulation
  * itself is computed and discarded. */
 int wtet_learned_collect(const float* xyz, const uint64_t* offsets, uint32_t num_clouds,

@@ -41,7 +41,7 @@ class _Config(ctypes.Structure):
         ("overlap_shift", ctypes.c_uint32),
         ("candidate_filter", ctypes.c_uint32),
         ("pool_factor", ctypes.c_uint32),
-        ("deep_threshold", ctypes.c_uint32),
+        ("learned_gate", ctypes.c_uint32),
         ("initial_capacity", ctypes.c_uint32),
         ("reserved", ctypes.c_uint32 * 1),
     ]
@@ -254,7 +254,7 @@ class Config:
                  enable_splaying: bool = True, max_insert_iterations: int = 100,
                  max_flip_iterations: int = 10, vote: str = "plain", block_size: int = 0,
                  rounds_per_graph: int = 0, overlap_shift: int = 0, candidate_filter: int = 0,
-                 pool_factor: int = 0, deep_threshold: int = 0, initial_capacity: int = 0):
+                 pool_factor: int = 0, learned_gate: int = 0, initial_capacity: int = 0):
         rule = str(insertion_rule).lower()
         if rule not in _RULES:
             raise ValueError(
@@ -275,7 +275,7 @@ class Config:
         self.overlap_shift = int(overlap_shift)
         self.candidate_filter = int(candidate_filter)
         self.pool_factor = int(pool_factor)
-        self.deep_threshold = int(deep_threshold)
+        self.learned_gate = int(learned_gate)
         self.initial_capacity = int(initial_capacity)
 
     def _c(self) -> _Config:
@@ -295,7 +295,7 @@ class Config:
         c.overlap_shift = self.overlap_shift
         c.candidate_filter = self.candidate_filter
         c.pool_factor = self.pool_factor
-        c.deep_threshold = self.deep_threshold
+        c.learned_gate = self.learned_gate
         c.initial_capacity = self.initial_capacity
         return c
 
@@ -426,11 +426,12 @@ def delaunay_batched(clouds, config: Config | None = None):
     return out
 
 
-def delaunay_device(points, config: Config | None = None):
+def delaunay_device(points, config: Config | None = None, with_stats: bool = False):
     """Zero-copy variant for a CUDA torch tensor of shape (N, 3), float32.
 
     Returns (tets, adjacency) as CUDA int32-viewed uint32 tensors of shape
-    (M, 4), computed on torch's current stream."""
+    (M, 4), computed on torch's current stream; with ``with_stats`` also the
+    call's statistics (the ``stats`` dict of DelaunayResult)."""
     import torch
 
     if not (isinstance(points, torch.Tensor) and points.is_cuda):
@@ -459,6 +460,8 @@ def delaunay_device(points, config: Config | None = None):
         break
     if rc != WTET_OK:
         _raise(rc)
+    if with_stats:
+        return tets[: m.value], adj[: m.value], st.as_dict()
     return tets[: m.value], adj[: m.value]
 
 

@@ -13,15 +13,16 @@
 // SoS Delaunay triangulation, with no flip failures and nothing left to repair.
 //
 // Round structure (one insertion round over all clouds of a job; 10 kernels
-// replayed from a CUDA graph, 11 with the learned scheduler):
+// replayed from a CUDA graph):
 //   k_activate    locate the new stratum's points (walk from the curve
 //                 predecessor's tet)
 //   k_vote        each uninserted point votes for its tet (64-bit atomicMax of
 //                 score | ~point, src/shaders/vote.wgsl semantics)
 //   k_cands       the winner of each tet becomes a candidate and pre-claims
-//                 its tet's neighbourhood with its claim key
-//   (k_sched      the learned scheduler decides which winners search this
-//                 round, with the fused BF16 MLP)
+//                 its tet's neighbourhood with its claim key (with the
+//                 learned scheduler, k_cands_learned: the fused BF16 MLP sets
+//                 the winners' claim priority in the rounds of the first
+//                 strata)
 //   k_bfs         candidates whose pre-claims all hold grow their cavities by
 //                 breadth-first search with exact insphere (16 lanes per
 //                 candidate), claiming cavity tets by 64-bit atomicMin of a
@@ -219,8 +220,8 @@ struct Dev {
   uint32_t vote_mode;
   uint8_t* losses;          // vote wins of each point that did not insert
   const mlp::Image* mlp;    // inference weights
-  uint8_t* defer;           // learned scheduler: the winner waits for the next round
-  float deep_threshold;     // learned scheduler: predicted insert probability below which it does
+  uint16_t* prio;           // learned scheduler: claim priority of this round's winners
+  uint32_t learned_points;  // rounds with at most this many uninserted points use the network
   float* log_x;             // logged features (log_cap x 12)
   uint8_t* log_y;           // logged labels: the winner inserted this round (1) or not (0)
   uint32_t* log_pslot;      // log record of each winner this round, NONE if not recorded
@@ -297,9 +298,10 @@ __device__ __forceinline__ uint32_t mix32(uint32_t h) {
 // keys win.  Huge-cavity candidates (bigflag 2, at most HUGE_SLOTS a round)
 // take priority 0: their cavities overlap many others, and at equal priority
 // they would wait until their whole neighbourhood is quiet.  Every other
-// candidate has priority 1.
+// candidate has priority 1, or with the learned scheduler the priority its
+// network gave it this round (1..1023).
 __device__ __forceinline__ unsigned long long make_key(const Dev& D, const RoundArgs& R, uint32_t p) {
-  const unsigned long long prio = D.bigflag[p] == 2 ? 0u : 1u;
+  const unsigned long long prio = D.bigflag[p] == 2 ? 0u : (D.prio ? D.prio[p] : 1u);
   return R.stamp | (prio << 32) | mix32(p ^ (R.round * 0x9E3779B9u));
 }
 
@@ -796,125 +798,42 @@ __device__ __forceinline__ uint32_t pre_claim_tet(const Dev& D, uint32_t t, uint
   return (nb2 == NONE || (nb2 >> 2) >= D.cap) ? NONE : nb2 >> 2;
 }
 
-// Pre-claim state of vote winner p in tet t0 after k_cands: lost1 -- a better
-// winner overwrote one of p's own pre-claims (t0 and its face neighbours),
-// so the plain filter skips p this round; better2 / any2 -- tets of p's
-// second ring (the other neighbours of its face neighbours) that hold a
-// better / any winner's pre-claim of this round; rivals -- face neighbours
-// that hold a vote winner.  (A claim record holds the pre-claim and the vote
-// in one sector.)
-__device__ __forceinline__ void filter_state(const Dev& D, const RoundArgs& R, uint32_t t0, unsigned long long key,
-                                             bool& lost1, uint32_t& better2, uint32_t& any2, uint32_t& rivals) {
-  lost1 = false;
-  better2 = any2 = rivals = 0;
-  const uint4 N = D.T[t0].n;
-  uint32_t nbt[4];
-  if (__ldcg(&D.C[t0].pre) != key) lost1 = true;
+// Features of vote winner p in its tet t (vote = the tet's vote word): the
+// tet's shape and the winner's place in it, how many of the face neighbours
+// and of the second ring hold a vote winner this round (a vote word is
+// cleared when its tet's points move on, so a non-zero word is this round's),
+// the winner's earlier failed wins and the round's scale.  k_cands has
+// already counted this win in losses[p].
+__device__ __forceinline__ void winner_features(const Dev& D, const RoundArgs& R, uint32_t p, uint32_t t,
+                                                unsigned long long vote, float* f) {
+  const uint4 V = D.T[t].v;
+  const uint4 N = D.T[t].n;
+  uint32_t r1 = 0, r2 = 0;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const uint32_t nb = comp(N, i);
-    nbt[i] = (nb == NONE || (nb >> 2) >= D.cap) ? NONE : nb;
-    if (nbt[i] == NONE) continue;
-    const Claim* c1 = &D.C[nb >> 2];
-    if (__ldcg(&c1->pre) != key) lost1 = true;
-    if (__ldcg(&c1->vote) != 0ull) ++rivals;
-  }
-  if (lost1) return;  // the plain filter skips this winner: no decision to make
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const uint32_t nb = nbt[i];
-    if (nb == NONE) continue;
+    if (nb == NONE || (nb >> 2) >= D.cap) continue;
+    if (__ldcg(&D.C[nb >> 2].vote) != 0ull) ++r1;
     const uint4 N2 = D.T[nb >> 2].n;
 #pragma unroll
-    for (int g = 1; g < 4; ++g) {
+    for (int g = 1; g < 4; ++g) {  // the three faces other than the one back to t
       const uint32_t nb2 = comp(N2, (int(nb & 3) + g) & 3);
-      if (nb2 == NONE || (nb2 >> 2) >= D.cap) continue;
-      const unsigned long long pv = __ldcg(&D.C[nb2 >> 2].pre);
-      if (this_round(R, pv)) {
-        ++any2;
-        if (pv < key) ++better2;
-      }
+      if (nb2 != NONE && (nb2 >> 2) < D.cap && __ldcg(&D.C[nb2 >> 2].vote) != 0ull) ++r2;
     }
   }
-}
-
-// Features of vote winner p in its tet t (vertices V); k_cands has already
-// counted this win in losses[p].
-__device__ __forceinline__ void winner_features(const Dev& D, const RoundArgs& R, uint32_t p, uint32_t t, uint4 V,
-                                                unsigned long long key, uint32_t better2, uint32_t any2,
-                                                uint32_t rivals, float* f) {
-  const float4 q = D.pts[p];
-  const float depth = vote_score(D.pts, V, q, 0);
   const uint32_t lost = D.losses[p] ? D.losses[p] - 1u : 0u;
-  const float priority = float(uint32_t(key)) * 2.3283064e-10f;  // hash / 2^32
-  mlp::features(D.pts[V.x], D.pts[V.y], D.pts[V.z], D.pts[V.w], q, depth, lost, R.round, priority, better2, any2,
-                rivals, f);
+  const uint32_t stratum = __ldcg(&D.st->stratum_size);
+  mlp::features(D.pts[V.x], D.pts[V.y], D.pts[V.z], D.pts[V.w], D.pts[p], __uint_as_float(uint32_t(vote >> 32)),
+                r1, r2, R.round, lost, R.n_active, stratum, f);
 }
 
-// Learned scheduler, after k_cands: a vote winner that passes the plain
-// pre-claim filter but finds a better winner's pre-claim in its second ring
-// often loses its cavity to that winner after a full (wasted) search -- but
-// not always: skipping all of them saves a third of the searches and adds
-// rounds.  The fused tensor-core MLP scores the winners (32 per warp,
-// consecutive in the start list) with the predicted probability that they
-// insert this round; those of the second-ring case predicted below
-// deep_threshold wait for the next round (k_bfs skips them).
-__global__ void __launch_bounds__(128) k_sched(Dev D) {
-  const RoundArgs R = load_round(D);
-  if (!R.live) return;
-  constexpr int RS = mlp::kRowStride;
-  __shared__ __align__(16) mlp::Smem S;
-  __shared__ __align__(16) uint32_t rows[4][32 * RS];
-  __shared__ float outs[4][32];
-  __shared__ uint32_t sp[kOrderBuckets + 2];
-  mlp::load_image(S, D.mlp);
-  load_start_prefix(D, sp);
-  const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t nstart = sp[kOrderBuckets + 1];
-  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-  for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + w) * 32; base < nstart; base += warps * 32) {
-    const uint32_t i = base + lane;
-    const bool valid = i < nstart;
-    uint32_t p = 0;
-    bool blocked = false;
-    float f[mlp::kIn];
-#pragma unroll
-    for (int k = 0; k < mlp::kIn; ++k) f[k] = 0.f;
-    bool lost1 = false;
-    if (valid) {
-      p = start_at(D, sp, i);
-      const uint32_t t = D.loc[p];
-      const unsigned long long key = make_key(D, R, p);
-      uint32_t better2, any2, rivals;
-      filter_state(D, R, t, key, lost1, better2, any2, rivals);
-      blocked = !lost1 && better2 > 0;
-      if (blocked) winner_features(D, R, p, t, D.T[t].v, key, better2, any2, rivals, f);
-    }    // the warp scores only if one of its winners needs a decision
-    if (__any_sync(0xFFFFFFFFu, blocked)) {
-      mlp::stage_row(rows[w] + lane * RS, f);
-      __syncwarp();
-      mlp::score32(S, rows[w], outs[w]);
-    }
-    if (valid) {
-      bool defer = lost1 && D.prefilter;  // the plain filter's decision, taken here for k_bfs
-      if (blocked) {
-        float sc = outs[w][lane];
-        sc = (sc == sc) ? fminf(fmaxf(sc, -20.f), 20.f) : -20.f;
-        defer = 1.f / (1.f + __expf(-sc)) < D.deep_threshold;
-      }
-      D.defer[p] = defer ? 1 : 0;
-    }
-    __syncwarp();
-  }
-}
-
-// Scheduler log, after k_cands: features of 1 in 2^log_shift of the winners
-// the learned scheduler decides on (they pass the plain filter and a better
-// winner pre-claimed part of their second ring); label 0 here, set to 1 by
-// k_write when the winner inserts this round.
+// Scheduler log (training data), after k_cands: in the rounds the learned
+// scheduler serves (at most learned_points uninserted points), the features
+// of 1 in 2^log_shift of the vote winners; label 0 here, set to 1 by k_write
+// when the winner inserts in this round.
 __global__ void k_log_features(Dev D) {
   const RoundArgs R = load_round(D);
-  if (!R.live) return;
+  if (!R.live || R.n_active > D.learned_points) return;
   __shared__ uint32_t sp[kOrderBuckets + 2];
   load_start_prefix(D, sp);
   const uint32_t nstart = sp[kOrderBuckets + 1];
@@ -922,38 +841,47 @@ __global__ void k_log_features(Dev D) {
     const uint32_t p = start_at(D, sp, s);
     D.log_pslot[p] = NONE;
     if ((mix32(p ^ (R.round * 0x27D4EB2Fu)) & ((1u << D.log_shift) - 1u)) != 0u) continue;
-    const uint32_t t = D.loc[p];
-    const unsigned long long key = make_key(D, R, p);
-    bool lost1;
-    uint32_t better2, any2, rivals;
-    filter_state(D, R, t, key, lost1, better2, any2, rivals);
-    if (lost1 || better2 == 0) continue;
     const uint32_t slot = atomicAdd(&D.st->log_used, 1u);
     if (slot >= D.log_cap) continue;
     D.log_pslot[p] = slot;
     D.log_y[slot] = 0;
+    const uint32_t t = D.loc[p];
     float f[mlp::kIn];
-    winner_features(D, R, p, t, D.T[t].v, key, better2, any2, rivals, f);
+    winner_features(D, R, p, t, __ldcg(&D.C[t].vote), f);
 #pragma unroll
     for (int k = 0; k < mlp::kIn; ++k) D.log_x[size_t(slot) * mlp::kIn + k] = f[k];
   }
 }
 
+// Shared memory of the learned candidate kernel: the network's weights and
+// one staged feature row per lane.
+constexpr uint32_t kCandWarps = 8;  // k_cands_learned runs 256-thread blocks
+struct CandSmem {
+  mlp::Smem S;
+  uint32_t rows[kCandWarps][32 * mlp::kRowStride];
+  float outs[kCandWarps][32];
+};
 
-// Candidates: the vote winner of each tet.  Points whose cavity outgrew the
-// warp scratch in an earlier round go to the huge-cavity path.
-__global__ void k_cands(Dev D) {
-  const RoundArgs R = load_round(D);
-  if (!R.live) return;
+// Candidates: the vote winner of each tet (the reference's pick_winner_point
+// and build_insert_list, src/shaders/vote.wgsl:508-616).  Points whose cavity
+// outgrew the warp scratch in an earlier round go to the huge-cavity path.
+// With kLearned, the fused network scores the warp's winners and sets their
+// claim priority; the start list is bucketed by that priority (better first)
+// instead of by the claim hash.
+template <bool kLearned>
+__device__ __forceinline__ void cands_body(const Dev& D, const RoundArgs& R, CandSmem* sm) {
+  const uint32_t lane = threadIdx.x & 31u;
   for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < R.n_active; i0 += gridDim.x * blockDim.x) {
     const uint32_t i = i0 + threadIdx.x;
     bool start = false;
-    uint32_t p = 0;
+    uint32_t p = 0, t = 0;
+    unsigned long long vote = 0;
     if (i < R.n_active) {
       p = R.active[i];
       const uint8_t tier = D.bigflag[p];
-      const uint32_t t = D.loc[p];
-      if (!(tier & kDup) && t < D.cap && uint32_t(D.C[t].vote) == ~p) {
+      t = D.loc[p];
+      if (!(tier & kDup) && t < D.cap) vote = D.C[t].vote;
+      if (!(tier & kDup) && t < D.cap && uint32_t(vote) == ~p) {
         if (D.losses && D.losses[p] < 255u) D.losses[p] += 1u;
         if (tier == 2) {
           uint32_t b = atomicAdd(&D.ctr->huge_used, 1u);
@@ -962,14 +890,40 @@ __global__ void k_cands(Dev D) {
           start = true;
           D.st1[p] = 0;
           D.st2[p] = 0;
-          if (D.prefilter) pre_claim(D, t, make_key(D, R, p), false);
         }
       }
     }
+    uint32_t b = 0;
+    if constexpr (kLearned) {
+      // the warp scores only if one of its points is a winner (warp-uniform)
+      if (__any_sync(0xFFFFFFFFu, start)) {
+        const uint32_t w = threadIdx.x >> 5;
+        float f[mlp::kIn];
+#pragma unroll
+        for (int k = 0; k < mlp::kIn; ++k) f[k] = 0.f;
+        if (start) winner_features(D, R, p, t, vote, f);
+        mlp::stage_row(sm->rows[w] + lane * mlp::kRowStride, f);
+        __syncwarp();
+        mlp::score32(sm->S, sm->rows[w], sm->outs[w]);
+        if (start) {
+          float sc = sm->outs[w][lane];
+          sc = (sc == sc) ? fminf(fmaxf(sc, -20.f), 20.f) : 0.f;
+          // predicted probability of inserting under hashed keys: the least
+          // likely (crowded neighbourhoods) claim first
+          const float pr = 1.f / (1.f + __expf(-sc));
+          const uint32_t prio = 1u + uint32_t(fminf(pr * 1022.f + 0.5f, 1022.f));
+          D.prio[p] = uint16_t(prio);
+          b = prio >> 6;  // 16 order buckets
+        }
+        __syncwarp();
+      }
+    } else {
+      if (start && D.prio) D.prio[p] = 1;
+      b = (start && D.exp_order) ? (mix32(p ^ (R.round * 0x9E3779B9u)) >> 28) : 0u;
+    }
+    if (start && D.prefilter) pre_claim(D, t, make_key(D, R, p), false);
     warp_append(&D.ctr->big_used, start);  // total count
-    const uint32_t b = (start && D.exp_order) ? (mix32(p ^ (R.round * 0x9E3779B9u)) >> 28) : 0u;
     const unsigned grp = __match_any_sync(0xFFFFFFFFu, start ? b : 0xFFFFFFFFu);
-    const uint32_t lane = threadIdx.x & 31u;
     const uint32_t leader = uint32_t(__ffs(grp) - 1);
     uint32_t base = 0;
     if (start && lane == leader) base = atomicAdd(&D.ctr->sbc[b], uint32_t(__popc(grp)));
@@ -983,6 +937,22 @@ __global__ void k_cands(Dev D) {
       }
     }
   }
+}
+
+__global__ void k_cands(Dev D) {
+  const RoundArgs R = load_round(D);
+  if (!R.live) return;
+  cands_body<false>(D, R, nullptr);
+}
+
+// The learned scheduler's candidate kernel (256-thread blocks).
+__global__ void __launch_bounds__(256) k_cands_learned(Dev D) {
+  const RoundArgs R = load_round(D);
+  if (!R.live) return;
+  __shared__ __align__(16) CandSmem sm;
+  mlp::load_image(sm.S, D.mlp);
+  __syncthreads();
+  cands_body<true>(D, R, &sm);
 }
 
 // Cavity growth by groups of kBfsLanes lanes, kWarpGroups candidates per
@@ -1052,15 +1022,13 @@ __global__ void __launch_bounds__(128, 8) k_bfs(Dev D) {
       pq = D.pts[p];
     }
     int pre_lost = 0;
-    if (active && D.prefilter && !D.defer) {
+    if (active && D.prefilter) {
       // the winner's own pre-claims (t0 and its face neighbours) must all hold
       for (uint32_t k = gl; k < 5; k += kBfsLanes) {
         const uint32_t t = pre_claim_tet(D, t0, k == 0 ? 0u : 4u * (k - 1u) + 1u);
         if (t != NONE && __ldcg(&D.C[t].pre) != key) pre_lost = 1;
       }
     }
-    // the learned scheduler deferred this winner to the next round
-    if (active && gl == 0 && D.defer && D.defer[p]) pre_lost = 1;
     // warp collectives first, outside any short-circuit: every lane must reach them
     const uint32_t g_pre = (__ballot_sync(FULL, pre_lost) >> shift) & GM;
     const bool searched = active && !g_pre;
@@ -2079,7 +2047,7 @@ struct Workspace {
   DBuf<uint8_t> dup;
   DBuf<uint32_t> log_pslot;
   DBuf<uint8_t> losses;
-  DBuf<uint8_t> defer;
+  DBuf<uint16_t> prio;
   std::vector<DBuf<uint32_t>> scan_tmp;
   Counters* h_ctr = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -2158,7 +2126,7 @@ void release_thread_workspace() {
   w.ccount.release(); w.hullcnt.release(); w.cfill.release(); w.newid.release();
   w.hull.release(); w.coff.release(); w.out_t.release(); w.out_a.release(); w.dtab.release(); w.dup.release();
   w.etab_key.release(); w.etab_val.release(); w.btab_key.release(); w.btab_val.release();
-  w.log_pslot.release(); w.losses.release(); w.defer.release();
+  w.log_pslot.release(); w.losses.release(); w.prio.release();
   for (auto& b : w.scan_tmp) b.release();
   if (w.h_ctr) cudaFreeHost(w.h_ctr);
   if (w.ev0) cudaEventDestroy(w.ev0);
@@ -2442,10 +2410,10 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     W.log_pslot.reserve(nv, "log slots");
     ck(cudaMemsetAsync(W.log_pslot.p, 0xFF, nv * 4, s), "memset");
   }
-  if (vmode == 1) {
-    W.defer.reserve(nv, "deferred winners");
-    ck(cudaMemsetAsync(W.defer.p, 0, nv, s), "memset");
-  }
+  if (vmode == 1) W.prio.reserve(nv, "claim priorities");
+  // Rounds whose graph may see at most this many uninserted points use the
+  // learned scheduler (its training log records the same rounds).
+  const uint64_t learned_points = uint64_t(cfg.learned_gate ? cfg.learned_gate : 2048u) * 1024u;
 
   Dev D{};
   auto refresh = [&]() {
@@ -2470,8 +2438,8 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     D.vote_mode = vmode;
     D.losses = vmode ? W.losses.p : nullptr;
     D.mlp = mlp_w;
-    D.defer = vmode == 1 ? W.defer.p : nullptr;
-    D.deep_threshold = (cfg.deep_threshold ? float(cfg.deep_threshold) : 64.f) / 256.f;
+    D.prio = vmode == 1 ? W.prio.p : nullptr;
+    D.learned_points = uint32_t(std::min<uint64_t>(learned_points, 0xFFFFFFFFull));
     D.log_x = job.d_log_x;
     D.log_y = job.d_log_y;
     D.log_pslot = vmode == 2 ? W.log_pslot.p : nullptr;
@@ -2549,25 +2517,27 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   // wave per kernel.
   const uint32_t GB = HUGE_SLOTS;  // one block per huge-cavity slot
   struct Grids {
-    uint32_t act, vote, cand, sched, logf, bfs, res, sh, wr, rel;
+    uint32_t act, vote, cand, candl, logf, bfs, res, sh, wr, rel;
   };
-  const Grids big{wave(k_activate, TB), wave(k_vote, TB),      wave(k_cands, TB),  wave(k_sched, 128),
+  const Grids big{wave(k_activate, TB), wave(k_vote, TB),      wave(k_cands, TB),
+                  vmode == 1 ? wave(k_cands_learned, 256) : 0u,
                   wave(k_log_features, TB), wave(k_bfs, 128), wave(k_resolve, 128), wave(k_shared, 128),
                   wave(k_write, 128),  wave(k_relocate, TB)};
   // Rounds of the first strata have a few thousand points: a full wave of
   // blocks that exit at once costs more than their work, so those rounds
   // replay a graph with one block per SM.
   auto shrink = [](uint32_t g) { return std::min<uint32_t>(g, 148u); };
-  const Grids small{shrink(big.act), shrink(big.vote), shrink(big.cand), shrink(big.sched), shrink(big.logf),
+  const Grids small{shrink(big.act), shrink(big.vote), shrink(big.cand), shrink(big.candl), shrink(big.logf),
                     shrink(big.bfs), shrink(big.res),  shrink(big.sh),   shrink(big.wr),    shrink(big.rel)};
-  const uint64_t kernels_per_round = 10 + (vmode ? 1 : 0);
+  const uint64_t kernels_per_round = 10 + (vmode == 2 ? 1 : 0);
 
   // One round: k_end also starts the next round (k_begin starts the first).
-  auto enqueue_round = [&](const Grids& G) {
+  // `learned`: the learned scheduler's candidate kernel.
+  auto enqueue_round = [&](const Grids& G, bool learned) {
     k_activate<<<G.act, TB, 0, s>>>(D);
     k_vote<<<G.vote, TB, 0, s>>>(D);
-    k_cands<<<G.cand, TB, 0, s>>>(D);
-    if (vmode == 1) k_sched<<<G.sched, 128, 0, s>>>(D);
+    if (learned) k_cands_learned<<<G.candl, 256, 0, s>>>(D);
+    else k_cands<<<G.cand, TB, 0, s>>>(D);
     if (vmode == 2) k_log_features<<<G.logf, TB, 0, s>>>(D);
     k_bfs<<<G.bfs, 128, 0, s>>>(D);
     k_expand_big<<<GB, 256, 0, s>>>(D);
@@ -2580,27 +2550,31 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   // Rounds per host check (the graph holds this many rounds).
   uint32_t rpg = std::min<uint32_t>(cfg.rounds_per_graph, 64u);
   if (trace) rpg = 1;
-  cudaGraphExec_t gexec = nullptr, gexec_small = nullptr;
-  auto capture = [&](const Grids& G) {
+  // Three graphs: the first strata's rounds (one block per SM), the bulk
+  // rounds (full waves), and with the learned scheduler the rounds in between
+  // (full waves, learned candidate kernel).
+  cudaGraphExec_t gexec = nullptr, gexec_small = nullptr, gexec_mid = nullptr;
+  auto capture = [&](const Grids& G, bool learned) {
     cudaGraph_t g = nullptr;
     cudaGraphExec_t e = nullptr;
     ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
-    for (uint32_t r = 0; r < rpg; ++r) enqueue_round(G);
+    for (uint32_t r = 0; r < rpg; ++r) enqueue_round(G, learned);
     ck(cudaStreamEndCapture(s, &g), "end capture");
     ck(cudaGraphInstantiate(&e, g, 0), "graph instantiate");
     cudaGraphDestroy(g);
     return e;
   };
-  auto build_graph = [&]() {
-    if (gexec) cudaGraphExecDestroy(gexec);
-    if (gexec_small) cudaGraphExecDestroy(gexec_small);
-    gexec = capture(big);
-    gexec_small = capture(small);
-  };
   auto destroy_graphs = [&]() {
     if (gexec) cudaGraphExecDestroy(gexec);
     if (gexec_small) cudaGraphExecDestroy(gexec_small);
-    gexec = gexec_small = nullptr;
+    if (gexec_mid) cudaGraphExecDestroy(gexec_mid);
+    gexec = gexec_small = gexec_mid = nullptr;
+  };
+  auto build_graph = [&]() {
+    destroy_graphs();
+    gexec = capture(big, false);
+    gexec_small = capture(small, vmode == 1);
+    if (vmode == 1) gexec_mid = capture(big, true);
   };
   // Points the next graph launch may see: the current list and the next two
   // strata (each stratum about doubles the previous one).
@@ -2621,7 +2595,10 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   }
   for (;;) {
     if (trace) ck(cudaEventRecord(tr0, s), "event record");
-    ck(cudaGraphLaunch(upcoming(hs) <= kSmallRoundPoints ? gexec_small : gexec, s), "graph launch");
+    const uint64_t u = upcoming(hs);
+    ck(cudaGraphLaunch(u <= kSmallRoundPoints ? gexec_small : (gexec_mid && u <= learned_points) ? gexec_mid : gexec,
+                       s),
+       "graph launch");
     if (trace) ck(cudaEventRecord(tr1, s), "event record");
     launches += uint64_t(rpg) * kernels_per_round;
     ck(cudaMemcpyAsync(&hs, W.state.p, sizeof(State), cudaMemcpyDeviceToHost, s), "d2h");

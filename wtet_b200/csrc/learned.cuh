@@ -1,26 +1,29 @@
 // Learned insertion scheduler: per vote-winner features and the fused BF16
-// MLP that predicts whether a vote winner will insert this round.
+// MLP that sets the claim priority of the vote winners.
 //
 // The reference orders insertions by the circumsphere determinant alone
 // (src/shaders/vote.wgsl:401-494); it has no learned scheduler.  Here every
-// tet still votes for the point deepest in its circumsphere, and each winner
-// pre-claims its tet and face neighbours; a winner whose pre-claims a better
-// one overwrote skips its cavity search this round (the plain method).  A
-// winner that passes but finds a better winner's pre-claim in its second ring
-// of neighbours often loses its cavity later, after a wasted search -- but
-// not always: skipping all of them saves a third of the searches and costs
-// rounds.  The network (12 -> 64 -> 64 -> 64 -> 1, ReLU, BF16 weights and
-// activations, FP32 accumulate; trained on the plain method's own logs)
-// predicts, for those winners, whether they would insert anyway; the ones
-// predicted to fail wait for the next round.  Only the order changes: every
-// round still inserts an exactly Delaunay-compatible set of points, so the
-// final tet set is the same unique SoS triangulation.
+// tet still votes for the point deepest in its circumsphere; the vote winners
+// then compete for their cavities by claim keys, and the one with the smaller
+// key wins a contested tet.  With hashed keys (the plain method) the winners
+// of a crowded neighbourhood lose to each other round after round, and those
+// neighbourhoods set the number of rounds.  The network (12 -> 64 -> 64 -> 64
+// -> 1, ReLU, BF16 weights and activations, FP32 accumulate; trained on the
+// plain method's own logs) predicts each winner's probability of inserting in
+// this round under hashed keys; winners predicted least likely to insert --
+// the crowded ones -- claim first.  It is used in the rounds of the first
+// strata, which cost a fixed overhead per round whatever their size; the
+// bulk rounds, where the work per round dominates, keep hashed keys.  Only
+// the order changes: every round still inserts an exactly
+// Delaunay-compatible set of points, so the final tet set is the same unique
+// SoS triangulation.
 //
 // Inference runs on the tensor cores with warp-level mma.m16n8k16 (BF16 in,
-// FP32 accumulate): each warp scores 32 winners at a time, the activations
-// stay in registers between layers (an accumulator fragment of one layer is
-// the A fragment of the next), and the weights sit in shared memory with
-// padded rows so that every fragment load is bank-conflict free.
+// FP32 accumulate), fused into the kernel that turns votes into winners: each
+// warp scores its 32 points at once, the activations stay in registers
+// between layers (an accumulator fragment of one layer is the A fragment of
+// the next), and the weights sit in shared memory with padded rows so that
+// every fragment load is bank-conflict free.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -177,15 +180,15 @@ __device__ __forceinline__ float finite_or(float x, float dflt) { return isfinit
 __device__ __forceinline__ float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
 
 // The 12 features of vote winner q in tet (a, b, c, d), all O(1) by construction:
-//  0 |q - circumcenter|^2 / R^2          6 claim priority of q this round (0 = best, 1 = worst)
-//  1 log2(insphere depth) / 64           7 second-ring tets pre-claimed by a better winner / 12
-//  2 6*sqrt(2)*V / emax^3 (1 = regular)  8 face-neighbour tets holding a vote winner / 4
-//  3 log2(R / emax) / 4                  9 share of the second ring's winners that are better
-//  4 second-ring tets pre-claimed by any winner / 12   10 log2(1 + earlier wins of q that did not insert) / 4
-//  5 log2(1 + round) / 8                11 tet has a super vertex
-__device__ __forceinline__ void features(float4 a, float4 b, float4 c, float4 d, float4 q, float depth,
-                                         uint32_t losses, uint32_t round, float priority, uint32_t better2,
-                                         uint32_t any2, uint32_t rivals, float* f) {
+//  0 |q - circumcenter|^2 / R^2            6 log2(1 + round) / 8
+//  1 log2(vote score) / 64                 7 log2(1 + earlier wins of q that did not insert) / 4
+//  2 6*sqrt(2)*V / emax^3 (1 = regular)    8 uninserted points / points of the last stratum, / 2
+//  3 log2(R / emax) / 4                    9 log2(1 + uninserted points) / 24
+//  4 face-neighbour tets holding a winner / 4          10 -log2(emax) / 16 (tet size)
+//  5 second-ring tets holding a winner / 12            11 the tet has a super vertex
+__device__ __forceinline__ void features(float4 a, float4 b, float4 c, float4 d, float4 q, float score,
+                                         uint32_t rivals1, uint32_t rivals2, uint32_t round, uint32_t losses,
+                                         uint32_t n_active, uint32_t stratum, float* f) {
   const float abx = b.x - a.x, aby = b.y - a.y, abz = b.z - a.z;
   const float acx = c.x - a.x, acy = c.y - a.y, acz = c.z - a.z;
   const float adx = d.x - a.x, ady = d.y - a.y, adz = d.z - a.z;
@@ -212,16 +215,16 @@ __device__ __forceinline__ void features(float4 a, float4 b, float4 c, float4 d,
   const bool sup = a.x < -50.f || a.x > 200.f || b.x < -50.f || b.x > 200.f || c.x < -50.f || c.x > 200.f ||
                    d.x < -50.f || d.x > 200.f;
   f[0] = clampf(finite_or((qx * qx + qy * qy + qz * qz) / R2, 1.f), 0.f, 1.f);
-  f[1] = clampf(finite_or(__log2f(depth + 1e-37f), -128.f) * (1.f / 64.f), -2.f, 2.f);
+  f[1] = clampf(finite_or(__log2f(score + 1e-37f), -128.f) * (1.f / 64.f), -2.f, 2.f);
   f[2] = clampf(finite_or(av6 * 1.41421356f / (emax2 * emax), 0.f), 0.f, 1.f);
   f[3] = clampf(finite_or(0.5f * __log2f(R2 / emax2), 8.f), -8.f, 8.f) * 0.25f;
-  f[4] = float(any2) * (1.f / 12.f);
-  f[5] = __log2f(1.f + float(round)) * 0.125f;
-  f[6] = priority;
-  f[7] = float(better2) * (1.f / 12.f);
-  f[8] = float(rivals) * 0.25f;
-  f[9] = any2 ? float(better2) / float(any2) : 0.f;
-  f[10] = __log2f(1.f + float(losses)) * 0.25f;
+  f[4] = float(rivals1) * 0.25f;
+  f[5] = float(rivals2) * (1.f / 12.f);
+  f[6] = __log2f(1.f + float(round)) * 0.125f;
+  f[7] = __log2f(1.f + float(losses)) * 0.25f;
+  f[8] = clampf(float(n_active) / float(max(stratum, 1u)), 0.f, 2.f) * 0.5f;
+  f[9] = __log2f(1.f + float(n_active)) * (1.f / 24.f);
+  f[10] = clampf(finite_or(-__log2f(emax), 0.f) * (1.f / 16.f), -1.f, 2.f);
   f[11] = sup ? 1.f : 0.f;
 }
 

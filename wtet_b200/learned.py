@@ -1,23 +1,25 @@
 """Learned insertion scheduler: data collection, training and weights.
 
 Every tet votes for its uninserted point deepest inside its circumsphere (the
-reference's vote, src/shaders/vote.wgsl:401-494).  Each vote winner then
-pre-claims its tet and face neighbours, and a winner whose pre-claims a
-better winner overwrote skips its cavity search this round (the plain
-method).  A winner that passes this filter but finds a better winner's
-pre-claim in its second ring often loses its cavity to that winner after a
-full, wasted search -- but not always, and skipping all of them costs rounds.
-``Config(vote="learned")`` lets a small MLP (12 -> 64 -> 64 -> 64 -> 1, ReLU)
-predict, for those winners, whether they would insert this round anyway; the
-ones predicted to fail wait for the next round.  Inference is fused into the
-kernel that schedules the winners (BF16 tensor-core mma, FP32 accumulate);
-the triangulation is unchanged, only the order of insertions.
+reference's vote, src/shaders/vote.wgsl:401-494).  The vote winners then
+compete for their cavities by claim keys: the smaller key wins a contested
+tet.  The plain method hashes the keys, so in a crowded neighbourhood the
+winners lose to each other round after round, and those neighbourhoods set
+the number of rounds.  ``Config(vote="learned")`` lets a small MLP (12 -> 64
+-> 64 -> 64 -> 1, ReLU) predict each winner's probability of inserting in
+this round under hashed keys; the winners least likely to insert -- the
+crowded ones -- get the smallest keys and claim first.  The network serves
+the rounds of the first strata (up to ``Config.learned_gate`` x 1024
+uninserted points), whose cost is a fixed overhead per round; the bulk
+rounds keep hashed keys.  Inference is fused into the kernel that turns
+votes into winners (BF16 tensor-core mma, FP32 accumulate); the
+triangulation is unchanged, only the order of insertions.
 
 Everything here runs on the GPU through libwtet.so:
 
 * ``collect``  -- training records from the plain method's own runs: the
-  features of sampled winners of that second-ring case and whether each
-  one inserted in its round;
+  features of sampled vote winners of the rounds the network serves and
+  whether each one inserted in its round;
 * ``train``    -- the project's forward / backward / Adam kernels;
 * ``loss_grad`` -- one forward + backward pass (checked against a CPU
   restatement in the tests);
@@ -36,16 +38,16 @@ from . import _core
 
 FEATURES = (
     "circumcenter_distance",   # |q - c|^2 / R^2
-    "insphere_depth",          # log2 of the plain vote's circumsphere depth / 64
+    "vote_score",              # log2 of the plain vote's score (circumsphere depth) / 64
     "volume_ratio",            # 6 sqrt(2) V / emax^3
     "circumradius_ratio",      # log2(R / emax) / 4
-    "second_ring_winners",     # second-ring tets pre-claimed by any winner / 12
-    "round",                   # log2(1 + round) / 8
-    "claim_priority",          # the winner's claim hash this round / 2^32 (0 = best)
-    "better_second_ring",      # second-ring tets pre-claimed by a better winner / 12
     "rival_neighbours",        # face-neighbour tets holding a vote winner / 4
-    "better_share",            # share of the second ring's winners that are better
+    "second_ring_winners",     # second-ring tets holding a vote winner / 12
+    "round",                   # log2(1 + round) / 8
     "failed_attempts",         # log2(1 + earlier vote wins without insertion) / 4
+    "stratum_progress",        # uninserted points / points of the last stratum, / 2
+    "round_scale",             # log2(1 + uninserted points) / 24
+    "tet_size",                # -log2(emax) / 16
     "super_vertex",            # the tet has a super vertex
 )
 NUM_FEATURES = 12
@@ -125,10 +127,9 @@ def load_default(path: str = DEFAULT_WEIGHTS) -> np.ndarray:
 def collect(clouds, config: _core.Config | None = None, capacity: int | None = None, sample_shift: int = 0):
     """Training records (X (m, 12) float32, y (m,) uint8, stats) from the
     plain method's run on ``clouds`` (list of (N, 3) arrays): features of 1 in
-    2**sample_shift of the vote winners the learned scheduler decides on (they
-    pass the plain pre-claim filter and a better winner pre-claimed part of
-    their second ring), and whether each one inserted in its round (1) or not
-    (0)."""
+    2**sample_shift of the vote winners in the rounds the learned scheduler
+    serves (at most ``config.learned_gate`` x 1024 uninserted points), and
+    whether each one inserted in its round (1) or not (0)."""
     arrs = [_core._points(c) for c in clouds]
     offsets = np.zeros(len(arrs) + 1, np.uint64)
     offsets[1:] = np.cumsum([a.shape[0] for a in arrs])
@@ -202,8 +203,9 @@ def training_clouds(seeds=(1, 2, 3, *range(11, 31)), size: int = 200_000):
     """The training distribution, from the small plain, degenerate and large
     plain configurations: per seed a 100k uniform cloud, a mixture cloud, a
     thin shell and a unit sphere (``size`` points, halved for the last two),
-    2M-point mixture clouds from four of the seeds, and exact lattices of
-    32^3, 48^3 and 64^3 points."""
+    2M-point mixture clouds from four of the seeds, 8M-point mixture clouds
+    from three (the network serves the first strata, whose size grows with
+    the cloud), and exact lattices of 32^3, 48^3 and 64^3 points."""
     from . import synthetic as syn
 
     for s in seeds:
@@ -213,6 +215,8 @@ def training_clouds(seeds=(1, 2, 3, *range(11, 31)), size: int = 200_000):
         yield [syn.unit_sphere(size // 2, s)]
     for s in seeds[3:7]:
         yield [syn.mixture(2_000_000, s)]
+    for s in seeds[:3]:
+        yield [syn.mixture(8_000_000, s)]
     for k in (32, 48, 64):
         yield [syn.lattice(k)]
 
