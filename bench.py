@@ -392,13 +392,16 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
-# DRAM bytes (read + write) of one whole triangulation: ncu launch list of one
-# 8M-mixture triangulation with dram__bytes_read.sum + dram__bytes_write.sum
-# (a one-pass metric set, so every launch is captured unreplayed), summed over
-# all launches.  Measured on the kernels of the revision named beside it; a
-# kernel change needs a new capture (profiles/ holds the summary and command).
-TRAFFIC: dict = {}
-TRAFFIC_SOURCE = ""
+# DRAM bytes (read + write) of one whole triangulation of the 8M mixture,
+# estimated with ncu: for each round kernel, the DRAM bytes per microsecond of
+# one launch in the most expensive round of the 1M mixture (one kernel, one
+# launch per capture) times that kernel's total time in the time-only launch
+# list of one 8M triangulation.  It describes the kernels it was measured on
+# and must be captured again when they change.
+TRAFFIC: dict = {"mixture8M": 311.8e9}
+TRAFFIC_SOURCE = ("estimate: sum over k_bfs, k_shared, k_write, k_cands, k_vote, k_relocate, k_activate of "
+                  "(DRAM bytes per us of one bulk-round launch on the 1M mixture, ncu) x (the kernel's total time "
+                  "in the 8M launch list, ncu); early rounds fit in L2, so this over-counts them")
 
 WORKLOADS = {
     "mixture8M": "8,000,000 points: 60% uniform [0,1]^3, 30% Gaussian ball (0.5, sigma 0.1), "

@@ -66,6 +66,22 @@
 #include "order.cuh"
 #include "devbuf.cuh"
 
+// Resident blocks per SM the round kernels are compiled for (register caps):
+// more resident warps hide more of the dependent-load latency, fewer
+// registers spill more.
+#ifndef WTET_BFS_MINB
+#define WTET_BFS_MINB 8
+#endif
+#ifndef WTET_SHARED_MINB
+#define WTET_SHARED_MINB 8
+#endif
+#ifndef WTET_WRITE_MINB
+#define WTET_WRITE_MINB 8
+#endif
+#ifndef WTET_RELOC_MINB
+#define WTET_RELOC_MINB 1
+#endif
+
 namespace wtet {
 
 constexpr uint32_t NONE = 0xFFFFFFFFu;
@@ -633,7 +649,7 @@ __global__ void k_init_clouds(const CloudInfo* ci, uint32_t nc, Dev D) {
 // stride earlier on the Morton curve (a point of an earlier stratum: its tet
 // once inserted, else the tet that still contains it).  The located points are
 // appended to the uninserted list at position `base`.
-__global__ void __launch_bounds__(512, 2) k_activate(Dev D) {
+__global__ void __launch_bounds__(512, WTET_RELOC_MINB) k_activate(Dev D) {
   RoundArgs R = load_round(D);
   if (!R.live) return;
   volatile State* S = D.st;
@@ -982,7 +998,7 @@ __device__ __forceinline__ unsigned long long ld_cg_u64(const unsigned long long
   return v;
 }
 
-__global__ void __launch_bounds__(128, 8) k_bfs(Dev D) {
+__global__ void __launch_bounds__(128, WTET_BFS_MINB) k_bfs(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
   constexpr uint32_t FULL = 0xFFFFFFFFu, GM = (kBfsLanes == 32) ? 0xFFFFFFFFu : ((1u << kBfsLanes) - 1u);
@@ -1297,7 +1313,7 @@ __device__ __forceinline__ uint32_t edge_hi(const uint4& V, int f, int k) {
 // tets).  The worse one of a violating pair steps back.  A winner that stays
 // is handed one slot per boundary face (recycled slots first, then fresh
 // ones) in the same pass over its cavity.
-__global__ void __launch_bounds__(128, 8) k_shared(Dev D) {
+__global__ void __launch_bounds__(128, WTET_SHARED_MINB) k_shared(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
   constexpr uint32_t FULL = 0xFFFFFFFFu;
@@ -1460,7 +1476,7 @@ __device__ __forceinline__ uint32_t edge_hash(uint32_t a, uint32_t b, uint32_t m
   return mix32(a * 0x9E3779B9u ^ b) & mask;
 }
 
-__global__ void __launch_bounds__(128, 8) k_write(Dev D) {
+__global__ void __launch_bounds__(128, WTET_WRITE_MINB) k_write(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
   __shared__ unsigned long long ekey[4][kEdgeSlots];
@@ -1698,7 +1714,7 @@ __global__ void __launch_bounds__(128, 8) k_write(Dev D) {
 // Clears the votes, relocates points whose tet was retired, compacts the
 // uninserted list, and carries the recycled slots that were not handed out
 // this round over to the next round's list.
-__global__ void __launch_bounds__(512, 2) k_relocate(Dev D) {
+__global__ void __launch_bounds__(512, WTET_RELOC_MINB) k_relocate(Dev D) {
   const RoundArgs R = load_round(D);
   if (!R.live) return;
   uint32_t steps = 0;
