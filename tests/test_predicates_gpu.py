@@ -5,7 +5,10 @@ records built to sit on every boundary between the stages: random points,
 near-coplanar and near-cospherical sets a rounding away from degenerate, exact
 lattice sets (SoS decides), tiny clusters whose permanents fall below the
 FP32 stage's underflow guard, and the reference's super-vertex coordinates
-(src/gpu/mod.rs:151-158)."""
+(src/gpu/mod.rs:151-158).  Exactly degenerate sets are decided by the
+modular exact stage (residues mod 2^64 and 2^61 - 1), near misses by its
+Chinese-remainder sign or by the expansion stage when its bound does not
+hold."""
 import numpy as np
 import pytest
 
@@ -32,6 +35,15 @@ def records(seed=7):
     # exact lattice picks: coplanar and cospherical sets, SoS decides
     lat = (r.integers(0, 4, (n, 5, 3)) / np.float32(4)).astype(np.float32)
     out.append(lat)
+    # the 128^3 benchmark lattice (f32(i / 127), not dyadic): corners of
+    # random boxes are exactly cospherical, faces exactly coplanar; the
+    # modular exact stage decides these (and CRT signs of near misses)
+    lo = r.integers(0, 120, (n, 1, 3))
+    ext = r.integers(1, 8, (n, 1, 3))
+    corner = r.integers(0, 2, (n, 5, 3))
+    box = ((lo + corner * ext).astype(np.float64) / 127.0).astype(np.float32)
+    out.append(box)
+    out.append((r.integers(0, 128, (n, 5, 3)).astype(np.float64) / 127.0).astype(np.float32))
     # tiny clusters: permanents below the FP32 stage's guard
     base = r.random((n // 2, 1, 3))
     out.append((base + 1e-7 * r.random((n // 2, 5, 3))).astype(np.float32))

@@ -287,6 +287,197 @@ constexpr double kO3dBoundA = (7.0 + 56.0 * kEps) * kEps;
 constexpr double kIspBoundA = (16.0 + 224.0 * kEps) * kEps;
 constexpr double kO3dBoundLifted = (11.0 + 112.0 * kEps) * kEps;  // src/predicates.rs:426-427
 
+// ---- Exact stage by modular arithmetic ----
+//
+// Every finite double is a dyadic rational m * 2^e (m odd).  With S the
+// smallest e among the coordinates of a predicate's points, every coordinate
+// is an integer multiple of 2^S, and orient3d / insphere -- homogeneous
+// polynomials of degree 3 / 5 in the coordinate differences with integer
+// coefficients -- equal det_int * 2^(3S) / det_int * 2^(5S) for the same
+// polynomial evaluated on the integers X = x / 2^S.  The stage evaluates that
+// polynomial in the residue rings Z / 2^64 and Z / P (P = 2^61 - 1, a Mersenne
+// prime) and reconstructs det_int by the Chinese remainder theorem, which is
+// exact for |det_int| < 2^64 P / 2 (about 2^124).  The bound comes from the
+// FP64 filter that ran first: when it cannot decide, |det_fp| <= err, so the
+// exact determinant is at most 2 err and |det_int| <= 2 err 2^(-dS).  The
+// stage answers only when that bound is below 2^122 and S >= -160 (points of
+// f32 origin, where the filter's bound is valid: no product of differences
+// reaches the FP64 underflow range); otherwise the expansion stage decides.
+// On exactly degenerate inputs -- cospherical corners of lattice boxes,
+// coplanar lattice faces -- it replaces hundreds of expansion operations by
+// about forty residue products.
+constexpr uint64_t kP61 = (1ull << 61) - 1ull;
+
+struct Res {  // a value mod 2^64 and mod P
+  uint64_t a, b;
+};
+__device__ __forceinline__ uint64_t mod_p(uint64_t x) {
+  x = (x & kP61) + (x >> 61);
+  return x >= kP61 ? x - kP61 : x;
+}
+__device__ __forceinline__ uint64_t mulmod_p(uint64_t x, uint64_t y) {
+  const uint64_t lo = x * y, hi = __umul64hi(x, y);  // x, y < 2^61: the product has < 122 bits
+  const uint64_t r = (lo & kP61) + ((hi << 3) | (lo >> 61));
+  return mod_p(r);
+}
+__device__ __forceinline__ Res radd(Res x, Res y) { return {x.a + y.a, mod_p(x.b + y.b)}; }
+__device__ __forceinline__ Res rsub(Res x, Res y) { return {x.a - y.a, mod_p(x.b + (kP61 - y.b))}; }
+__device__ __forceinline__ Res rmul(Res x, Res y) { return {x.a * y.a, mulmod_p(x.b, y.b)}; }
+
+// x = (-1)^neg m 2^e with m odd (m = 0 for zero).  Finite inputs only.
+__device__ __forceinline__ void dyadic(double x, uint64_t& m, int& e, bool& neg) {
+  const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(x));
+  neg = (bits >> 63) != 0;
+  const int be = int((bits >> 52) & 0x7FF);
+  m = bits & ((1ull << 52) - 1ull);
+  if (be != 0) m |= 1ull << 52;
+  e = (be != 0 ? be : 1) - 1075;
+  if (m == 0) {
+    e = 1 << 20;  // never the minimum
+    return;
+  }
+  const int tz = __ffsll(static_cast<long long>(m)) - 1;
+  m >>= tz;
+  e += tz;
+}
+
+// Residues of x / 2^S (an integer: e >= S).
+__device__ __forceinline__ Res residue(uint64_t m, int e, bool neg, int S) {
+  if (m == 0) return {0ull, 0ull};
+  const int k = e - S;
+  const uint64_t a = k < 64 ? (m << k) : 0ull;
+  const uint64_t b = mulmod_p(mod_p(m), 1ull << (k % 61));
+  return neg ? Res{0ull - a, b ? kP61 - b : 0ull} : Res{a, b};
+}
+
+// Sign of the integer with residues r, known to satisfy |x| < 2^123.
+__device__ __forceinline__ int crt_sign(Res r) {
+  // x = r.a + 2^64 k with k = (r.b - r.a) / 2^64 mod P; 2^64 = 8 mod P and
+  // 1/8 = 2^58 mod P.
+  const uint64_t k = mulmod_p(mod_p(r.b + (kP61 - mod_p(r.a))), 1ull << 58);
+  if (k == 0) return r.a == 0 ? 0 : 1;
+  // x in [0, 2^64 P): negative when at least half the modulus
+  const unsigned __int128 x = (static_cast<unsigned __int128>(k) << 64) | r.a;
+  const unsigned __int128 half = static_cast<unsigned __int128>(kP61) << 63;
+  return x >= half ? -1 : 1;
+}
+
+// Exact sign of Shewchuk's orient3d / insphere on the points' integer
+// multiples of 2^S, or 2 when the stage does not apply.  `err` is the FP64
+// filter's bound for the same points (the filter could not decide).
+__device__ __noinline__ int orient3d_modular(const double* pa, const double* pb, const double* pc,
+                                             const double* pd, double err) {
+  const double* P[4] = {pa, pb, pc, pd};
+  uint64_t m[12];
+  int e[12];
+  bool ng[12];
+  int S = 1 << 20;
+#pragma unroll
+  for (int i = 0; i < 12; ++i) {
+    dyadic(P[i / 3][i % 3], m[i], e[i], ng[i]);
+    S = min(S, e[i]);
+  }
+  if (S == (1 << 20)) return 0;  // all coordinates zero
+  if (S < -160 || !(ldexp(2.0 * err * (1.0 + 0x1p-40), -3 * S) < 0x1p122)) return 2;
+  Res X[12];
+#pragma unroll
+  for (int i = 0; i < 12; ++i) X[i] = residue(m[i], e[i], ng[i], S);
+  const Res adx = rsub(X[0], X[9]), ady = rsub(X[1], X[10]), adz = rsub(X[2], X[11]);
+  const Res bdx = rsub(X[3], X[9]), bdy = rsub(X[4], X[10]), bdz = rsub(X[5], X[11]);
+  const Res cdx = rsub(X[6], X[9]), cdy = rsub(X[7], X[10]), cdz = rsub(X[8], X[11]);
+  const Res det = radd(radd(rmul(adz, rsub(rmul(bdx, cdy), rmul(cdx, bdy))),
+                            rmul(bdz, rsub(rmul(cdx, ady), rmul(adx, cdy)))),
+                       rmul(cdz, rsub(rmul(adx, bdy), rmul(bdx, ady))));
+  return crt_sign(det);
+}
+
+__device__ __noinline__ int insphere_modular(const double* pa, const double* pb, const double* pc,
+                                             const double* pd, const double* pe, double err) {
+  const double* P[5] = {pa, pb, pc, pd, pe};
+  uint64_t m[15];
+  int e[15];
+  bool ng[15];
+  int S = 1 << 20;
+#pragma unroll
+  for (int i = 0; i < 15; ++i) {
+    dyadic(P[i / 3][i % 3], m[i], e[i], ng[i]);
+    S = min(S, e[i]);
+  }
+  if (S == (1 << 20)) return 0;
+  if (S < -160 || !(ldexp(2.0 * err * (1.0 + 0x1p-40), -5 * S) < 0x1p122)) return 2;
+  Res X[15];
+#pragma unroll
+  for (int i = 0; i < 15; ++i) X[i] = residue(m[i], e[i], ng[i], S);
+  const Res aex = rsub(X[0], X[12]), aey = rsub(X[1], X[13]), aez = rsub(X[2], X[14]);
+  const Res bex = rsub(X[3], X[12]), bey = rsub(X[4], X[13]), bez = rsub(X[5], X[14]);
+  const Res cex = rsub(X[6], X[12]), cey = rsub(X[7], X[13]), cez = rsub(X[8], X[14]);
+  const Res dex = rsub(X[9], X[12]), dey = rsub(X[10], X[13]), dez = rsub(X[11], X[14]);
+  const Res ab = rsub(rmul(aex, bey), rmul(bex, aey)), bc = rsub(rmul(bex, cey), rmul(cex, bey));
+  const Res cd = rsub(rmul(cex, dey), rmul(dex, cey)), da = rsub(rmul(dex, aey), rmul(aex, dey));
+  const Res ac = rsub(rmul(aex, cey), rmul(cex, aey)), bd = rsub(rmul(bex, dey), rmul(dex, bey));
+  const Res abc = radd(rsub(rmul(aez, bc), rmul(bez, ac)), rmul(cez, ab));
+  const Res bcd = radd(rsub(rmul(bez, cd), rmul(cez, bd)), rmul(dez, bc));
+  const Res cda = radd(radd(rmul(cez, da), rmul(dez, ac)), rmul(aez, cd));
+  const Res dab = radd(radd(rmul(dez, ab), rmul(aez, bd)), rmul(bez, da));
+  const Res al = radd(radd(rmul(aex, aex), rmul(aey, aey)), rmul(aez, aez));
+  const Res bl = radd(radd(rmul(bex, bex), rmul(bey, bey)), rmul(bez, bez));
+  const Res cl = radd(radd(rmul(cex, cex), rmul(cey, cey)), rmul(cez, cez));
+  const Res dl = radd(radd(rmul(dex, dex), rmul(dey, dey)), rmul(dez, dez));
+  const Res det = radd(rsub(rmul(dl, abc), rmul(cl, dab)), rsub(rmul(bl, cda), rmul(al, bcd)));
+  return crt_sign(det);
+}
+
+// Exact sign of det[[p_0, p_1, |p|^2, 1]] over rows a..d (the lifted
+// orient3d's exact stage), or 2 when the stage does not apply.  Subtracting
+// row d gives the 3x3 determinant of (du, dv, |p|^2 - |d|^2) over rows a..c,
+// which is evaluated on the residues.  Its magnitude is bounded from the
+// coordinates: the permanent of (|du|, |dv|, sum_j |p_j - d_j| |p_j + d_j|)
+// in FP64, with a margin for its own rounding.
+__device__ __noinline__ int lifted_modular(const double* pa, const double* pb, const double* pc,
+                                           const double* pd) {
+  const double* P[4] = {pa, pb, pc, pd};
+  uint64_t m[12];
+  int e[12];
+  bool ng[12];
+  int S = 1 << 20;
+#pragma unroll
+  for (int i = 0; i < 12; ++i) {
+    dyadic(P[i / 3][i % 3], m[i], e[i], ng[i]);
+    S = min(S, e[i]);
+  }
+  if (S == (1 << 20)) return 0;
+  if (S < -160) return 2;
+  double du[3], dv[3], dl[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    du[r] = fabs(P[r][0] - pd[0]);
+    dv[r] = fabs(P[r][1] - pd[1]);
+    dl[r] = fabs(P[r][0] - pd[0]) * fabs(P[r][0] + pd[0]) + fabs(P[r][1] - pd[1]) * fabs(P[r][1] + pd[1]) +
+            fabs(P[r][2] - pd[2]) * fabs(P[r][2] + pd[2]);
+  }
+  const double perm = du[0] * (dv[1] * dl[2] + dv[2] * dl[1]) + du[1] * (dv[0] * dl[2] + dv[2] * dl[0]) +
+                      du[2] * (dv[0] * dl[1] + dv[1] * dl[0]);
+  if (!(ldexp(perm * (1.0 + 0x1p-30), -4 * S) < 0x1p122)) return 2;
+  Res X[12];
+#pragma unroll
+  for (int i = 0; i < 12; ++i) X[i] = residue(m[i], e[i], ng[i], S);
+  Res L[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+    L[r] = radd(radd(rmul(X[3 * r], X[3 * r]), rmul(X[3 * r + 1], X[3 * r + 1])), rmul(X[3 * r + 2], X[3 * r + 2]));
+  Res U[3], V[3], W[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    U[r] = rsub(X[3 * r], X[9]);
+    V[r] = rsub(X[3 * r + 1], X[10]);
+    W[r] = rsub(L[r], L[3]);
+  }
+  const Res det = radd(rsub(rmul(U[0], rsub(rmul(V[1], W[2]), rmul(V[2], W[1]))),
+                            rmul(U[1], rsub(rmul(V[0], W[2]), rmul(V[2], W[0])))),
+                       rmul(U[2], rsub(rmul(V[0], W[1]), rmul(V[1], W[0]))));
+  return crt_sign(det);
+}
+
 // Sign of Shewchuk orient3d(a,b,c,d): FP64 filter, then exact.
 __device__ __forceinline__ int orient3d(const double* pa, const double* pb, const double* pc, const double* pd,
                                         uint32_t* flags) {
@@ -302,10 +493,12 @@ __device__ __forceinline__ int orient3d(const double* pa, const double* pb, cons
   double err = kO3dBoundA * perm;
   if (det > err) return 1;
   if (-det > err) return -1;
-  // Fresh copies for the out-of-line exact stage: the caller's coordinate
+  // Fresh copies for the out-of-line exact stages: the caller's coordinate
   // arrays never have their address taken, so they stay in registers.
   double a[3] = {pa[0], pa[1], pa[2]}, b[3] = {pb[0], pb[1], pb[2]};
   double c[3] = {pc[0], pc[1], pc[2]}, d[3] = {pd[0], pd[1], pd[2]};
+  const int sm = orient3d_modular(a, b, c, d, err);
+  if (sm != 2) return sm;
   return orient3d_exact_sign(a, b, c, d, flags);
 }
 
@@ -342,6 +535,8 @@ __device__ __forceinline__ int insphere(const double* pa, const double* pb, cons
   double a[3] = {pa[0], pa[1], pa[2]}, b[3] = {pb[0], pb[1], pb[2]};
   double c[3] = {pc[0], pc[1], pc[2]}, d[3] = {pd[0], pd[1], pd[2]};
   double e[3] = {pe[0], pe[1], pe[2]};
+  const int sm = insphere_modular(a, b, c, d, e, err);
+  if (sm != 2) return sm;
   return insphere_exact_sign(a, b, c, d, e, flags);
 }
 
@@ -455,6 +650,8 @@ __device__ __noinline__ int orient3d_lifted(const double* a0, const double* b0, 
                 (fabs(adxbdy) + fabs(bdxady)) * fabs(cdz);
   double err = kO3dBoundLifted * perm;
   if (det > err || -det > err) return (det > 0.0) - (det < 0.0);
+  const int sm = lifted_modular(pa, pb, pc, pd);
+  if (sm != 2) return sm;
   int kl[4];
   double K[4][6];
   kl[0] = lift(pa, K[0]);
