@@ -3,11 +3,10 @@
 ``python -m wtet_b200.build`` compiles the CUDA sources in ``csrc/`` with
 nvcc for ``arch=compute_100a,code=sm_100a`` into ``wtet_b200/libwtet.so``
 (in-tree, so the library travels with the repository).  Each source is its
-own object, compiled in parallel.  The sources that evaluate the exact
-predicates (EXACT_SOURCES) are compiled with ``-fmad=false``: the filters,
-expansions and the reference's SoS arithmetic rely on separately rounded
-products and sums.  The others (the scheduler network's training and scoring
-kernels, the C ABI) keep FMA contraction.
+own object, compiled in parallel, with the compiler's default contraction of
+multiplies and adds: the exact predicates (exact.cuh, the FP32 stage of the
+round kernels and the normalisation) spell every operation whose rounding
+matters as a separately rounded intrinsic.
 """
 from __future__ import annotations
 
@@ -22,7 +21,7 @@ LIB = os.path.join(HERE, "libwtet.so")
 SOURCES = ["engine.cu", "capi.cu", "noalloc.cu", "learned.cu", "verify.cu"]
 HEADERS = ["exact.cuh", "engine.cuh", "learned.cuh", "order.cuh", "devbuf.cuh"]
 
-EXACT_SOURCES = {"engine.cu", "verify.cu", "noalloc.cu"}
+EXACT_SOURCES: set = set()  # sources that would need -fmad=false (none)
 
 NVCC_FLAGS = [
     "-O3",

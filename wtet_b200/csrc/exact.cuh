@@ -19,8 +19,9 @@
 // by cofactors), so it needs no exact coordinate differences.  The SoS
 // cascades reproduce the reference's arithmetic operation by operation,
 // including its plain-double orient2d and coordinate differences and its own
-// filtered lifted orient3d; this file must be compiled with -fmad=false so
-// that every product and sum is rounded on its own, as in the reference.
+// filtered lifted orient3d; every product and sum is a separately rounded
+// intrinsic, as in the reference, whatever the translation unit's
+// contraction setting.
 #pragma once
 #include <cstdint>
 
@@ -40,19 +41,29 @@ __device__ __forceinline__ void raise_precision(uint32_t* flags) {
   if (flags) atomicOr(flags, kErrPrecision);
 }
 
+// Every FP64 operation of this file is a separately rounded intrinsic
+// (__dadd_rn, __dsub_rn, __dmul_rn), which the compiler never contracts into
+// a fused multiply-add: the filters' error bounds, the expansion arithmetic
+// and the reference's plain-double SoS arithmetic all assume one rounding per
+// operation.  Only two_prod uses a fused multiply-add, for the exact error of
+// a product.
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+
 __device__ __forceinline__ void two_sum(double a, double b, double& x, double& y) {
-  x = a + b;
-  double bv = x - a;
-  double av = x - bv;
-  y = (a - av) + (b - bv);
+  x = dadd(a, b);
+  double bv = dsub(x, a);
+  double av = dsub(x, bv);
+  y = dadd(dsub(a, av), dsub(b, bv));
 }
 __device__ __forceinline__ void fast_two_sum(double a, double b, double& x, double& y) {
-  x = a + b;
-  y = b - (x - a);
+  x = dadd(a, b);
+  y = dsub(b, dsub(x, a));
 }
 // Exact product with one fused multiply-add for the rounding error.
 __device__ __forceinline__ void two_prod(double a, double b, double& x, double& y) {
-  x = a * b;
+  x = dmul(a, b);
   y = __fma_rn(a, b, -x);
 }
 
@@ -378,7 +389,7 @@ __device__ __noinline__ int orient3d_modular(const double* pa, const double* pb,
     S = min(S, e[i]);
   }
   if (S == (1 << 20)) return 0;  // all coordinates zero
-  if (S < -160 || !(ldexp(2.0 * err * (1.0 + 0x1p-40), -3 * S) < 0x1p122)) return 2;
+  if (S < -160 || !(ldexp(dmul(err, 2.0 + 0x1p-39), -3 * S) < 0x1p122)) return 2;
   Res X[12];
 #pragma unroll
   for (int i = 0; i < 12; ++i) X[i] = residue(m[i], e[i], ng[i], S);
@@ -404,7 +415,7 @@ __device__ __noinline__ int insphere_modular(const double* pa, const double* pb,
     S = min(S, e[i]);
   }
   if (S == (1 << 20)) return 0;
-  if (S < -160 || !(ldexp(2.0 * err * (1.0 + 0x1p-40), -5 * S) < 0x1p122)) return 2;
+  if (S < -160 || !(ldexp(dmul(err, 2.0 + 0x1p-39), -5 * S) < 0x1p122)) return 2;
   Res X[15];
 #pragma unroll
   for (int i = 0; i < 15; ++i) X[i] = residue(m[i], e[i], ng[i], S);
@@ -450,14 +461,15 @@ __device__ __noinline__ int lifted_modular(const double* pa, const double* pb, c
   double du[3], dv[3], dl[3];
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
-    du[r] = fabs(P[r][0] - pd[0]);
-    dv[r] = fabs(P[r][1] - pd[1]);
-    dl[r] = fabs(P[r][0] - pd[0]) * fabs(P[r][0] + pd[0]) + fabs(P[r][1] - pd[1]) * fabs(P[r][1] + pd[1]) +
-            fabs(P[r][2] - pd[2]) * fabs(P[r][2] + pd[2]);
+    du[r] = fabs(dsub(P[r][0], pd[0]));
+    dv[r] = fabs(dsub(P[r][1], pd[1]));
+    dl[r] = dadd(dadd(dmul(du[r], fabs(dadd(P[r][0], pd[0]))), dmul(dv[r], fabs(dadd(P[r][1], pd[1])))),
+                 dmul(fabs(dsub(P[r][2], pd[2])), fabs(dadd(P[r][2], pd[2]))));
   }
-  const double perm = du[0] * (dv[1] * dl[2] + dv[2] * dl[1]) + du[1] * (dv[0] * dl[2] + dv[2] * dl[0]) +
-                      du[2] * (dv[0] * dl[1] + dv[1] * dl[0]);
-  if (!(ldexp(perm * (1.0 + 0x1p-30), -4 * S) < 0x1p122)) return 2;
+  const double perm = dadd(dadd(dmul(du[0], dadd(dmul(dv[1], dl[2]), dmul(dv[2], dl[1]))),
+                                dmul(du[1], dadd(dmul(dv[0], dl[2]), dmul(dv[2], dl[0])))),
+                           dmul(du[2], dadd(dmul(dv[0], dl[1]), dmul(dv[1], dl[0]))));
+  if (!(ldexp(dmul(perm, 1.0 + 0x1p-30), -4 * S) < 0x1p122)) return 2;
   Res X[12];
 #pragma unroll
   for (int i = 0; i < 12; ++i) X[i] = residue(m[i], e[i], ng[i], S);
@@ -481,16 +493,18 @@ __device__ __noinline__ int lifted_modular(const double* pa, const double* pb, c
 // Sign of Shewchuk orient3d(a,b,c,d): FP64 filter, then exact.
 __device__ __forceinline__ int orient3d(const double* pa, const double* pb, const double* pc, const double* pd,
                                         uint32_t* flags) {
-  double adx = pa[0] - pd[0], bdx = pb[0] - pd[0], cdx = pc[0] - pd[0];
-  double ady = pa[1] - pd[1], bdy = pb[1] - pd[1], cdy = pc[1] - pd[1];
-  double adz = pa[2] - pd[2], bdz = pb[2] - pd[2], cdz = pc[2] - pd[2];
-  double bdxcdy = bdx * cdy, cdxbdy = cdx * bdy;
-  double cdxady = cdx * ady, adxcdy = adx * cdy;
-  double adxbdy = adx * bdy, bdxady = bdx * ady;
-  double det = adz * (bdxcdy - cdxbdy) + bdz * (cdxady - adxcdy) + cdz * (adxbdy - bdxady);
-  double perm = (fabs(bdxcdy) + fabs(cdxbdy)) * fabs(adz) + (fabs(cdxady) + fabs(adxcdy)) * fabs(bdz) +
-                (fabs(adxbdy) + fabs(bdxady)) * fabs(cdz);
-  double err = kO3dBoundA * perm;
+  double adx = dsub(pa[0], pd[0]), bdx = dsub(pb[0], pd[0]), cdx = dsub(pc[0], pd[0]);
+  double ady = dsub(pa[1], pd[1]), bdy = dsub(pb[1], pd[1]), cdy = dsub(pc[1], pd[1]);
+  double adz = dsub(pa[2], pd[2]), bdz = dsub(pb[2], pd[2]), cdz = dsub(pc[2], pd[2]);
+  double bdxcdy = dmul(bdx, cdy), cdxbdy = dmul(cdx, bdy);
+  double cdxady = dmul(cdx, ady), adxcdy = dmul(adx, cdy);
+  double adxbdy = dmul(adx, bdy), bdxady = dmul(bdx, ady);
+  double det = dadd(dadd(dmul(adz, dsub(bdxcdy, cdxbdy)), dmul(bdz, dsub(cdxady, adxcdy))),
+                    dmul(cdz, dsub(adxbdy, bdxady)));
+  double perm = dadd(dadd(dmul(dadd(fabs(bdxcdy), fabs(cdxbdy)), fabs(adz)),
+                          dmul(dadd(fabs(cdxady), fabs(adxcdy)), fabs(bdz))),
+                     dmul(dadd(fabs(adxbdy), fabs(bdxady)), fabs(cdz)));
+  double err = dmul(kO3dBoundA, perm);
   if (det > err) return 1;
   if (-det > err) return -1;
   // Fresh copies for the out-of-line exact stages: the caller's coordinate
@@ -505,31 +519,33 @@ __device__ __forceinline__ int orient3d(const double* pa, const double* pb, cons
 // Sign of Shewchuk insphere(a,b,c,d,e): FP64 filter, then exact.
 __device__ __forceinline__ int insphere(const double* pa, const double* pb, const double* pc, const double* pd,
                                         const double* pe, uint32_t* flags) {
-  double aex = pa[0] - pe[0], bex = pb[0] - pe[0], cex = pc[0] - pe[0], dex = pd[0] - pe[0];
-  double aey = pa[1] - pe[1], bey = pb[1] - pe[1], cey = pc[1] - pe[1], dey = pd[1] - pe[1];
-  double aez = pa[2] - pe[2], bez = pb[2] - pe[2], cez = pc[2] - pe[2], dez = pd[2] - pe[2];
-  double aexbey = aex * bey, bexaey = bex * aey, ab = aexbey - bexaey;
-  double bexcey = bex * cey, cexbey = cex * bey, bc = bexcey - cexbey;
-  double cexdey = cex * dey, dexcey = dex * cey, cd = cexdey - dexcey;
-  double dexaey = dex * aey, aexdey = aex * dey, da = dexaey - aexdey;
-  double aexcey = aex * cey, cexaey = cex * aey, ac = aexcey - cexaey;
-  double bexdey = bex * dey, dexbey = dex * bey, bd = bexdey - dexbey;
-  double abc = aez * bc - bez * ac + cez * ab;
-  double bcd = bez * cd - cez * bd + dez * bc;
-  double cda = cez * da + dez * ac + aez * cd;
-  double dab = dez * ab + aez * bd + bez * da;
-  double alift = aex * aex + aey * aey + aez * aez;
-  double blift = bex * bex + bey * bey + bez * bez;
-  double clift = cex * cex + cey * cey + cez * cez;
-  double dlift = dex * dex + dey * dey + dez * dez;
-  double det = (dlift * abc - clift * dab) + (blift * cda - alift * bcd);
+  double aex = dsub(pa[0], pe[0]), bex = dsub(pb[0], pe[0]), cex = dsub(pc[0], pe[0]), dex = dsub(pd[0], pe[0]);
+  double aey = dsub(pa[1], pe[1]), bey = dsub(pb[1], pe[1]), cey = dsub(pc[1], pe[1]), dey = dsub(pd[1], pe[1]);
+  double aez = dsub(pa[2], pe[2]), bez = dsub(pb[2], pe[2]), cez = dsub(pc[2], pe[2]), dez = dsub(pd[2], pe[2]);
+  double aexbey = dmul(aex, bey), bexaey = dmul(bex, aey), ab = dsub(aexbey, bexaey);
+  double bexcey = dmul(bex, cey), cexbey = dmul(cex, bey), bc = dsub(bexcey, cexbey);
+  double cexdey = dmul(cex, dey), dexcey = dmul(dex, cey), cd = dsub(cexdey, dexcey);
+  double dexaey = dmul(dex, aey), aexdey = dmul(aex, dey), da = dsub(dexaey, aexdey);
+  double aexcey = dmul(aex, cey), cexaey = dmul(cex, aey), ac = dsub(aexcey, cexaey);
+  double bexdey = dmul(bex, dey), dexbey = dmul(dex, bey), bd = dsub(bexdey, dexbey);
+  double abc = dadd(dsub(dmul(aez, bc), dmul(bez, ac)), dmul(cez, ab));
+  double bcd = dadd(dsub(dmul(bez, cd), dmul(cez, bd)), dmul(dez, bc));
+  double cda = dadd(dadd(dmul(cez, da), dmul(dez, ac)), dmul(aez, cd));
+  double dab = dadd(dadd(dmul(dez, ab), dmul(aez, bd)), dmul(bez, da));
+  double alift = dadd(dadd(dmul(aex, aex), dmul(aey, aey)), dmul(aez, aez));
+  double blift = dadd(dadd(dmul(bex, bex), dmul(bey, bey)), dmul(bez, bez));
+  double clift = dadd(dadd(dmul(cex, cex), dmul(cey, cey)), dmul(cez, cez));
+  double dlift = dadd(dadd(dmul(dex, dex), dmul(dey, dey)), dmul(dez, dez));
+  double det = dadd(dsub(dmul(dlift, abc), dmul(clift, dab)), dsub(dmul(blift, cda), dmul(alift, bcd)));
   double az = fabs(aez), bz = fabs(bez), cz = fabs(cez), dz = fabs(dez);
-  double p_ab = fabs(aexbey) + fabs(bexaey), p_bc = fabs(bexcey) + fabs(cexbey);
-  double p_cd = fabs(cexdey) + fabs(dexcey), p_da = fabs(dexaey) + fabs(aexdey);
-  double p_ac = fabs(aexcey) + fabs(cexaey), p_bd = fabs(bexdey) + fabs(dexbey);
-  double perm = (p_cd * bz + p_bd * cz + p_bc * dz) * alift + (p_da * cz + p_ac * dz + p_cd * az) * blift +
-                (p_ab * dz + p_bd * az + p_da * bz) * clift + (p_bc * az + p_ac * bz + p_ab * cz) * dlift;
-  double err = kIspBoundA * perm;
+  double p_ab = dadd(fabs(aexbey), fabs(bexaey)), p_bc = dadd(fabs(bexcey), fabs(cexbey));
+  double p_cd = dadd(fabs(cexdey), fabs(dexcey)), p_da = dadd(fabs(dexaey), fabs(aexdey));
+  double p_ac = dadd(fabs(aexcey), fabs(cexaey)), p_bd = dadd(fabs(bexdey), fabs(dexbey));
+  double perm = dadd(dadd(dadd(dmul(dadd(dadd(dmul(p_cd, bz), dmul(p_bd, cz)), dmul(p_bc, dz)), alift),
+                               dmul(dadd(dadd(dmul(p_da, cz), dmul(p_ac, dz)), dmul(p_cd, az)), blift)),
+                          dmul(dadd(dadd(dmul(p_ab, dz), dmul(p_bd, az)), dmul(p_da, bz)), clift)),
+                     dmul(dadd(dadd(dmul(p_bc, az), dmul(p_ac, bz)), dmul(p_ab, cz)), dlift));
+  double err = dmul(kIspBoundA, perm);
   if (det > err) return 1;
   if (-det > err) return -1;
   double a[3] = {pa[0], pa[1], pa[2]}, b[3] = {pb[0], pb[1], pb[2]};
@@ -626,7 +642,7 @@ __device__ __forceinline__ int insphere_f32(const float4& pa, const float4& pb, 
 // Plain double orient2d on coordinates (u, v): src/predicates.rs:73-75.
 __device__ __forceinline__ double orient2d_plain(const double* a, const double* b, const double* c, int u,
                                                  int v) {
-  return (a[u] - c[u]) * (b[v] - c[v]) - (a[v] - c[v]) * (b[u] - c[u]);
+  return dsub(dmul(dsub(a[u], c[u]), dsub(b[v], c[v])), dmul(dsub(a[v], c[v]), dsub(b[u], c[u])));
 }
 
 // Lifted orient3d on permuted coordinates: the reference's filter and error
@@ -637,18 +653,20 @@ __device__ __noinline__ int orient3d_lifted(const double* a0, const double* b0, 
   double pb[3] = {b0[q0], b0[q1], b0[q2]};
   double pc[3] = {c0[q0], c0[q1], c0[q2]};
   double pd[3] = {d0[q0], d0[q1], d0[q2]};
-  double adx = pa[0] - pd[0], bdx = pb[0] - pd[0], cdx = pc[0] - pd[0];
-  double ady = pa[1] - pd[1], bdy = pb[1] - pd[1], cdy = pc[1] - pd[1];
-  double adzr = pa[2] - pd[2], bdzr = pb[2] - pd[2], cdzr = pc[2] - pd[2];
-  double adz = adx * adx + ady * ady + adzr * adzr;
-  double bdz = bdx * bdx + bdy * bdy + bdzr * bdzr;
-  double cdz = cdx * cdx + cdy * cdy + cdzr * cdzr;
-  double bdxcdy = bdx * cdy, cdxbdy = cdx * bdy, cdxady = cdx * ady;
-  double adxcdy = adx * cdy, adxbdy = adx * bdy, bdxady = bdx * ady;
-  double det = adz * (bdxcdy - cdxbdy) + bdz * (cdxady - adxcdy) + cdz * (adxbdy - bdxady);
-  double perm = (fabs(bdxcdy) + fabs(cdxbdy)) * fabs(adz) + (fabs(cdxady) + fabs(adxcdy)) * fabs(bdz) +
-                (fabs(adxbdy) + fabs(bdxady)) * fabs(cdz);
-  double err = kO3dBoundLifted * perm;
+  double adx = dsub(pa[0], pd[0]), bdx = dsub(pb[0], pd[0]), cdx = dsub(pc[0], pd[0]);
+  double ady = dsub(pa[1], pd[1]), bdy = dsub(pb[1], pd[1]), cdy = dsub(pc[1], pd[1]);
+  double adzr = dsub(pa[2], pd[2]), bdzr = dsub(pb[2], pd[2]), cdzr = dsub(pc[2], pd[2]);
+  double adz = dadd(dadd(dmul(adx, adx), dmul(ady, ady)), dmul(adzr, adzr));
+  double bdz = dadd(dadd(dmul(bdx, bdx), dmul(bdy, bdy)), dmul(bdzr, bdzr));
+  double cdz = dadd(dadd(dmul(cdx, cdx), dmul(cdy, cdy)), dmul(cdzr, cdzr));
+  double bdxcdy = dmul(bdx, cdy), cdxbdy = dmul(cdx, bdy), cdxady = dmul(cdx, ady);
+  double adxcdy = dmul(adx, cdy), adxbdy = dmul(adx, bdy), bdxady = dmul(bdx, ady);
+  double det = dadd(dadd(dmul(adz, dsub(bdxcdy, cdxbdy)), dmul(bdz, dsub(cdxady, adxcdy))),
+                    dmul(cdz, dsub(adxbdy, bdxady)));
+  double perm = dadd(dadd(dmul(dadd(fabs(bdxcdy), fabs(cdxbdy)), fabs(adz)),
+                          dmul(dadd(fabs(cdxady), fabs(adxcdy)), fabs(bdz))),
+                     dmul(dadd(fabs(adxbdy), fabs(bdxady)), fabs(cdz)));
+  double err = dmul(kO3dBoundLifted, perm);
   if (det > err || -det > err) return (det > 0.0) - (det < 0.0);
   const int sm = lifted_modular(pa, pb, pc, pd);
   if (sm != 2) return sm;
@@ -772,15 +790,15 @@ __device__ __noinline__ int orient3d_sos_degenerate(const double* a, const doubl
       case 1: v = orient2d_plain(p[1], p[2], p[3], 0, 2); break;
       case 2: v = orient2d_plain(p[1], p[2], p[3], 1, 2); break;
       case 3: v = orient2d_plain(p[0], p[2], p[3], 0, 1); break;
-      case 4: v = p[2][0] - p[3][0]; break;
-      case 5: v = p[2][1] - p[3][1]; break;
+      case 4: v = dsub(p[2][0], p[3][0]); break;
+      case 5: v = dsub(p[2][1], p[3][1]); break;
       case 6: v = orient2d_plain(p[0], p[2], p[3], 0, 2); break;
-      case 7: v = p[2][2] - p[3][2]; break;
+      case 7: v = dsub(p[2][2], p[3][2]); break;
       case 8: v = orient2d_plain(p[0], p[2], p[3], 1, 2); break;
       case 9: v = orient2d_plain(p[0], p[1], p[3], 0, 1); break;
-      case 10: v = p[1][0] - p[3][0]; break;
-      case 11: v = p[1][1] - p[3][1]; break;
-      default: v = p[0][0] - p[3][0]; break;
+      case 10: v = dsub(p[1][0], p[3][0]); break;
+      case 11: v = dsub(p[1][1], p[3][1]); break;
+      default: v = dsub(p[0][0], p[3][0]); break;
     }
     if (v != 0.0) {
       r = v;
@@ -827,7 +845,7 @@ __device__ __noinline__ int orient4d_sos_degenerate(const double* a, const doubl
       }
       case kO2L: s = orient2d_lifted(x, y, z, L.q0); break;
       case kO1: {
-        double v = x[L.q0] - y[L.q0];
+        double v = dsub(x[L.q0], y[L.q0]);
         s = (v > 0.0) - (v < 0.0);
         break;
       }
