@@ -202,7 +202,6 @@ struct Dev {
   Claim* C;
   uint4* nslot;
   uint32_t* bface;  // boundary faces of this round's winners, (tet << 2) | face, per winner contiguous
-  uint32_t inplace; // small stars reuse their cavity's slots
   uint32_t cap;
   uint32_t nv;  // vertices (range guard)
   // clouds
@@ -219,7 +218,6 @@ struct Dev {
   uint32_t* starts;   // vote winners expanding their cavity this round, in order-bucket regions
   uint32_t start_rc;  // capacity of one order bucket's region
   uint32_t start_ovf; // offset of the overflow region
-  uint32_t exp_order, exp_bchunk;
   uint32_t prefilter;
   uint32_t* wscratch; // one BIG_CAP cavity queue per lane group of k_bfs
   unsigned long long* etab_key;  // k_write's global edge tables, kEdgeSlotsG per warp
@@ -375,11 +373,10 @@ __device__ __noinline__ int o3d_sos_slow(float4 a, float4 b, float4 c, float4 d,
   const double A[3] = {a.x, a.y, a.z}, B[3] = {b.x, b.y, b.z}, C[3] = {c.x, c.y, c.z}, Dd[3] = {d.x, d.y, d.z};
   return o3d_sos(A, B, C, Dd, va, vb, vc, vd, sos, err);
 }
-__device__ int g_exp_f32 = 1;
 __device__ __forceinline__ int o3d_sos_f(const float4& a, const float4& b, const float4& c, const float4& d,
                                          uint32_t va, uint32_t vb, uint32_t vc, uint32_t vd, const uint32_t* sos,
                                          uint32_t* err) {
-  const int s = g_exp_f32 ? ex::orient3d_f32(a, b, c, d) : 0;
+  const int s = ex::orient3d_f32(a, b, c, d);
   if (s != 0) return s < 0 ? 1 : -1;
   return o3d_sos_slow(a, b, c, d, va, vb, vc, vd, sos, err);
 }
@@ -393,7 +390,7 @@ __device__ __noinline__ int o4d_sos_slow(float4 a, float4 b, float4 c, float4 d,
 __device__ __forceinline__ int o4d_sos_f(const float4& a, const float4& b, const float4& c, const float4& d,
                                          const float4& e, uint32_t va, uint32_t vb, uint32_t vc, uint32_t vd,
                                          uint32_t ve, const uint32_t* sos, uint32_t* err) {
-  const int s = g_exp_f32 ? ex::insphere_f32(a, b, c, d, e) : 0;
+  const int s = ex::insphere_f32(a, b, c, d, e);
   if (s != 0) return s;
   return o4d_sos_slow(a, b, c, d, e, va, vb, vc, vd, ve, sos, err);
 }
@@ -935,7 +932,7 @@ __device__ __forceinline__ void cands_body(const Dev& D, const RoundArgs& R, Can
       }
     } else {
       if (start && D.prio) D.prio[p] = 1;
-      b = (start && D.exp_order) ? (mix32(p ^ (R.round * 0x9E3779B9u)) >> 28) : 0u;
+      b = start ? (mix32(p ^ (R.round * 0x9E3779B9u)) >> 28) : 0u;
     }
     if (start && D.prefilter) pre_claim(D, t, make_key(D, R, p), false);
     warp_append(&D.ctr->big_used, start);  // total count
@@ -1017,10 +1014,10 @@ __global__ void __launch_bounds__(128, WTET_BFS_MINB) k_bfs(Dev D) {
   load_start_prefix(D, sp);
   const uint32_t nstart = sp[kOrderBuckets + 1];
   unsigned long long searches = 0;
-  // Work is taken dynamically, kChunk x kWarpGroups consecutive starts per
-  // warp: cavities differ in size by orders of magnitude, and a static
-  // grid-stride split leaves warps idle behind the slowest ones.
-  const uint32_t bchunk = kWarpGroups * D.exp_bchunk;
+  // Work is taken dynamically, one start per lane group (kWarpGroups per
+  // warp) per fetch: cavities differ in size by orders of magnitude, and a
+  // static grid-stride split leaves warps idle behind the slowest ones.
+  const uint32_t bchunk = kWarpGroups;
   for (uint32_t chunk0 = warp_next(&D.ctr->work[0], bchunk); chunk0 < nstart;
        chunk0 = warp_next(&D.ctr->work[0], bchunk))
   for (uint32_t base = chunk0; base < min(chunk0 + bchunk, nstart); base += kWarpGroups) {
@@ -1380,7 +1377,7 @@ __global__ void __launch_bounds__(128, WTET_SHARED_MINB) k_shared(Dev D) {
       // takes the slot of cavity tet r), plus fresh slots for the faces
       // beyond K: tets that are neighbours in space stay neighbours in memory.
       // Larger stars take recycled / fresh slots for every face.
-      inpl[j] = D.inplace && total <= kInPlaceFaces && !(D.cand_off[ci] & 0x80000000u);
+      inpl[j] = total <= kInPlaceFaces && !(D.cand_off[ci] & 0x80000000u);
       keep[j] = true;
       need_total[j] = total;
       need_fresh[j] = total - (inpl[j] ? min(K, total) : 0u);
@@ -2307,10 +2304,6 @@ void reserve_stack_once() {
 
 JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t capacity) {
   reserve_stack_once();
-  {
-    int f = getenv("WTET_F32") ? atoi(getenv("WTET_F32")) : 1;
-    cudaMemcpyToSymbol(g_exp_f32, &f, sizeof(int));
-  }
   Workspace& W = ws();
   // The legacy default stream cannot be captured into a graph; the workspace's
   // own (blocking) stream orders with it implicitly.
@@ -2440,9 +2433,6 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     D.cand_len = W.cand_len.p; D.cand_base = W.cand_base.p; D.cand_nf = W.cand_nf.p; D.st1 = W.st1.p; D.st2 = W.st2.p; D.bigcand = W.bigcand.p;
     D.starts = W.starts.p; D.wscratch = W.wscratch.p;
     D.start_rc = uint32_t(start_rc); D.start_ovf = uint32_t(start_ovf);
-    D.exp_order = getenv("WTET_ORDER") ? uint32_t(atoi(getenv("WTET_ORDER"))) : 1u;
-    D.exp_bchunk = getenv("WTET_BCHUNK") ? uint32_t(atoi(getenv("WTET_BCHUNK"))) : 1u;
-    D.inplace = getenv("WTET_INPLACE") ? uint32_t(atoi(getenv("WTET_INPLACE"))) : 1u;
     D.etab_key = W.etab_key.p; D.etab_val = W.etab_val.p; D.etab_warps = etab_warps;
     D.btab_key = W.btab_key.p; D.btab_val = W.btab_val.p;
     D.prefilter = cfg.candidate_filter == 2 ? 0u : 1u; D.pool = W.pool.p; D.pool_cap = pool_cap; D.big = W.big.p;
