@@ -78,6 +78,9 @@
 #ifndef WTET_WRITE_MINB
 #define WTET_WRITE_MINB 8
 #endif
+#ifndef WTET_SHARED_TEST
+#define WTET_SHARED_TEST o4d_sos_call
+#endif
 #ifndef WTET_RELOC_MINB
 #define WTET_RELOC_MINB 1
 #endif
@@ -393,6 +396,14 @@ __device__ __forceinline__ int o4d_sos_f(const float4& a, const float4& b, const
   const int s = ex::insphere_f32(a, b, c, d, e);
   if (s != 0) return s;
   return o4d_sos_slow(a, b, c, d, e, va, vb, vc, vd, ve, sos, err);
+}
+
+// The same insphere test out of line (FP32 stage included), for kernels that
+// test a face only now and then: their main path then keeps fewer registers.
+__device__ __noinline__ int o4d_sos_call(float4 a, float4 b, float4 c, float4 d, float4 e, uint32_t va, uint32_t vb,
+                                         uint32_t vc, uint32_t vd, uint32_t ve, const uint32_t* sos,
+                                         uint32_t* err) {
+  return o4d_sos_f(a, b, c, d, e, va, vb, vc, vd, ve, sos, err);
 }
 
 // Visibility walk with exact orient3d + SoS from tet t to the tet containing p.
@@ -1359,7 +1370,7 @@ __global__ void __launch_bounds__(128, WTET_SHARED_MINB) k_shared(Dev D) {
               const uint4 V = D.T[c].v;
               const uint32_t w0 = f == 0 ? p : V.x, w1 = f == 1 ? p : V.y, w2 = f == 2 ? p : V.z,
                              w3 = f == 3 ? p : V.w;
-              if (o4d_sos_f(D.pts[w0], D.pts[w1], D.pts[w2], D.pts[w3], D.pts[q], w0, w1, w2, w3, q, D.sos,
+              if (WTET_SHARED_TEST(D.pts[w0], D.pts[w1], D.pts[w2], D.pts[w3], D.pts[q], w0, w1, w2, w3, q, D.sos,
                             &D.ctr->err) < 0)
                 bad = true;
             }
