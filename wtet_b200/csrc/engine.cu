@@ -78,6 +78,11 @@
 #ifndef WTET_WRITE_MINB
 #define WTET_WRITE_MINB 8
 #endif
+// Rounds whose graph may see at most this many uninserted points run with one
+// block per SM per kernel (a full wave of blocks costs more than their work).
+#ifndef WTET_SMALL_ROUND_POINTS
+#define WTET_SMALL_ROUND_POINTS 32768
+#endif
 #ifndef WTET_SHARED_TEST
 #define WTET_SHARED_TEST o4d_sos_call
 #endif
@@ -330,8 +335,14 @@ __device__ __forceinline__ uint32_t warp_next(uint32_t* cursor, uint32_t chunk) 
   return __shfl_sync(0xFFFFFFFFu, v, 0);
 }
 // Items are taken kChunk at a time: one shared cursor serves every warp of
-// the grid, and same-address atomics serialise in their L2 slice.
+// the grid, and same-address atomics serialise in their L2 slice.  A round
+// with fewer than kChunk items per warp takes them one at a time instead
+// (there, a chunk would make a few warps do all the work in sequence).
 constexpr uint32_t kChunk = 4;
+__device__ __forceinline__ uint32_t chunk_for(uint32_t items) {
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  return items >= kChunk * warps ? kChunk : 1u;
+}
 // Stars of at most this many tets are written into their own cavity's slots
 // (k_write holds one new tet per lane in registers until the warp has read
 // the whole cavity).
@@ -1327,7 +1338,8 @@ __global__ void __launch_bounds__(128, WTET_SHARED_MINB) k_shared(Dev D) {
   constexpr uint32_t FULL = 0xFFFFFFFFu;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t ncand = __ldcg(&D.ctr->n_cand);
-  for (uint32_t c0 = warp_next(&D.ctr->work[1], kChunk); c0 < ncand; c0 = warp_next(&D.ctr->work[1], kChunk)) {
+  const uint32_t ch = chunk_for(ncand);
+  for (uint32_t c0 = warp_next(&D.ctr->work[1], ch); c0 < ncand; c0 = warp_next(&D.ctr->work[1], ch)) {
     // Phase 1, per winner of the chunk: the shared-face test and the count of
     // boundary faces.  Phase 2: one allocation for the whole chunk (the slot
     // and list counters are shared by every warp of the grid).  Phase 3: the
@@ -1340,7 +1352,7 @@ __global__ void __launch_bounds__(128, WTET_SHARED_MINB) k_shared(Dev D) {
       keep[j] = false;
       inpl[j] = false;
       need_fresh[j] = need_total[j] = bmask[j] = 0;
-      if (ci >= ncand) continue;
+      if (j >= ch || ci >= ncand) continue;
       const uint32_t p = D.cand[ci];
       if (!D.st1[p]) {
         if (lane == 0) D.st2[p] = 0;
@@ -1502,8 +1514,9 @@ __global__ void __launch_bounds__(128, WTET_WRITE_MINB) k_write(Dev D) {
   __syncthreads();
   uint32_t inserted = 0;
   unsigned long long created = 0;
-  for (uint32_t c0 = warp_next(&D.ctr->work[2], kChunk); c0 < ncand; c0 = warp_next(&D.ctr->work[2], kChunk))
-  for (uint32_t ci = c0; ci < min(c0 + kChunk, ncand); ++ci) {
+  const uint32_t ch = chunk_for(ncand);
+  for (uint32_t c0 = warp_next(&D.ctr->work[2], ch); c0 < ncand; c0 = warp_next(&D.ctr->work[2], ch))
+  for (uint32_t ci = c0; ci < min(c0 + ch, ncand); ++ci) {
     uint32_t p = D.cand[ci];
     if (!D.st2[p]) continue;
     uint32_t K = D.cand_len[ci];
@@ -2600,7 +2613,7 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
     for (int L = h.next_level, k = 0; L >= 0 && k < 2; --L, ++k) u += lvl_total[L];
     return u;
   };
-  constexpr uint64_t kSmallRoundPoints = 32768;
+  constexpr uint64_t kSmallRoundPoints = WTET_SMALL_ROUND_POINTS;
   build_graph();
   k_begin<<<1, 32, 0, s>>>(D);
   launches += 1;
