@@ -144,11 +144,11 @@ def test_collect_records(gpu):
     assert set(np.unique(y)) == {0, 1}                     # inserted in its round, or not
     assert (X[:, 0] >= 0).all() and (X[:, 0] <= 1).all()   # circumcenter distance
     assert (X[:, 4] >= 0).all() and (X[:, 4] <= 1).all()   # rival neighbours / 4
-    assert (X[:, 5] >= 0).all() and (X[:, 5] <= 1).all()   # second-ring winners / 12
+    assert (X[:, 5] >= 0).all() and (X[:, 5] <= X[:, 4]).all()  # better-scored rivals among the rivals
     assert (X[:, 8] >= 0).all() and (X[:, 8] <= 1).all()   # stratum progress
     assert set(np.unique(X[:, 11])) <= {0.0, 1.0}          # super-vertex flag
     # a winner that shares its neighbourhood with other winners inserts less often
-    crowded = X[:, 4] + X[:, 5] > np.median(X[:, 4] + X[:, 5])
+    crowded = X[:, 4] > np.median(X[:, 4])
     assert y[crowded].mean() < y[~crowded].mean()
     # the gate: with a small one only the small rounds are recorded
     Xs, _, _ = learned.collect([pts], gpu.Config(learned_gate=1), sample_shift=0)

@@ -834,11 +834,11 @@ __device__ __forceinline__ uint32_t pre_claim_tet(const Dev& D, uint32_t t, uint
 }
 
 // Features of vote winner p in its tet t (vote = the tet's vote word): the
-// tet's shape and the winner's place in it, how many of the face neighbours
-// and of the second ring hold a vote winner this round (a vote word is
-// cleared when its tet's points move on, so a non-zero word is this round's),
-// the winner's earlier failed wins and the round's scale.  k_cands has
-// already counted this win in losses[p].
+// tet's shape and the winner's place in it, how many face neighbours hold a
+// vote winner this round (a vote word is cleared when its tet's points move
+// on, so a non-zero word is this round's) and how many of those winners have
+// a larger vote score, the winner's earlier failed wins and the round's
+// scale.  k_cands has already counted this win in losses[p].
 __device__ __forceinline__ void winner_features(const Dev& D, const RoundArgs& R, uint32_t p, uint32_t t,
                                                 unsigned long long vote, float* f) {
   const uint4 V = D.T[t].v;
@@ -848,13 +848,9 @@ __device__ __forceinline__ void winner_features(const Dev& D, const RoundArgs& R
   for (int i = 0; i < 4; ++i) {
     const uint32_t nb = comp(N, i);
     if (nb == NONE || (nb >> 2) >= D.cap) continue;
-    if (__ldcg(&D.C[nb >> 2].vote) != 0ull) ++r1;
-    const uint4 N2 = D.T[nb >> 2].n;
-#pragma unroll
-    for (int g = 1; g < 4; ++g) {  // the three faces other than the one back to t
-      const uint32_t nb2 = comp(N2, (int(nb & 3) + g) & 3);
-      if (nb2 != NONE && (nb2 >> 2) < D.cap && __ldcg(&D.C[nb2 >> 2].vote) != 0ull) ++r2;
-    }
+    const unsigned long long nv = __ldcg(&D.C[nb >> 2].vote);
+    if (nv != 0ull) ++r1;
+    if ((nv >> 32) > (vote >> 32)) ++r2;  // a rival with a larger vote score
   }
   const uint32_t lost = D.losses[p] ? D.losses[p] - 1u : 0u;
   const uint32_t stratum = __ldcg(&D.st->stratum_size);

@@ -185,7 +185,7 @@ __device__ __forceinline__ float clampf(float x, float lo, float hi) { return fm
 //  2 6*sqrt(2)*V / emax^3 (1 = regular)    8 uninserted points / points of the last stratum, / 2
 //  3 log2(R / emax) / 4                    9 log2(1 + uninserted points) / 24
 //  4 face-neighbour tets holding a winner / 4          10 -log2(emax) / 16 (tet size)
-//  5 second-ring tets holding a winner / 12            11 the tet has a super vertex
+//  5 of those, winners with a larger vote score / 4    11 the tet has a super vertex
 __device__ __forceinline__ void features(float4 a, float4 b, float4 c, float4 d, float4 q, float score,
                                          uint32_t rivals1, uint32_t rivals2, uint32_t round, uint32_t losses,
                                          uint32_t n_active, uint32_t stratum, float* f) {
@@ -219,7 +219,7 @@ __device__ __forceinline__ void features(float4 a, float4 b, float4 c, float4 d,
   f[2] = clampf(finite_or(av6 * 1.41421356f / (emax2 * emax), 0.f), 0.f, 1.f);
   f[3] = clampf(finite_or(0.5f * __log2f(R2 / emax2), 8.f), -8.f, 8.f) * 0.25f;
   f[4] = float(rivals1) * 0.25f;
-  f[5] = float(rivals2) * (1.f / 12.f);
+  f[5] = float(rivals2) * 0.25f;
   f[6] = __log2f(1.f + float(round)) * 0.125f;
   f[7] = __log2f(1.f + float(losses)) * 0.25f;
   f[8] = clampf(float(n_active) / float(max(stratum, 1u)), 0.f, 2.f) * 0.5f;

@@ -42,7 +42,7 @@ FEATURES = (
     "volume_ratio",            # 6 sqrt(2) V / emax^3
     "circumradius_ratio",      # log2(R / emax) / 4
     "rival_neighbours",        # face-neighbour tets holding a vote winner / 4
-    "second_ring_winners",     # second-ring tets holding a vote winner / 12
+    "better_rivals",           # of those winners, the ones with a larger vote score / 4
     "round",                   # log2(1 + round) / 8
     "failed_attempts",         # log2(1 + earlier vote wins without insertion) / 4
     "stratum_progress",        # uninserted points / points of the last stratum, / 2
