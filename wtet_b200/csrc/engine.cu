@@ -993,9 +993,12 @@ __global__ void __launch_bounds__(256) k_cands_learned(Dev D) {
 // several such chains in flight.  The queue starts in shared memory and
 // continues in the group's global region; cavities beyond BIG_CAP move to the
 // huge path next round.
-constexpr uint32_t kBfsLanes = 16;
+#ifndef WTET_BFS_LANES
+#define WTET_BFS_LANES 16
+#endif
+constexpr uint32_t kBfsLanes = WTET_BFS_LANES;
 constexpr uint32_t kWarpGroups = 32 / kBfsLanes;
-constexpr uint32_t kBfsShared = 64;  // queue entries (tet + neighbour words) per group in shared memory
+constexpr uint32_t kBfsShared = 4 * kBfsLanes;  // queue entries (tet + neighbour words) per group in shared memory
 
 // Loads issued as written (volatile asm is neither sunk into the branch that
 // uses the value nor merged with later loads), so that a pass of the cavity
@@ -1151,19 +1154,24 @@ __global__ void __launch_bounds__(128, WTET_BFS_MINB) k_bfs(Dev D) {
     // One reservation for the warp's completed cavities (pool entries and
     // candidate slots are shared counters of the whole grid).
     const uint32_t kk = ok ? K : 0u;
-    const uint32_t kk_lo = __shfl_sync(FULL, kk, 0), kk_hi = __shfl_sync(FULL, kk, kBfsLanes % 32);
-    const uint32_t n_ok = (kk_lo ? 1u : 0u) + (kWarpGroups > 1 && kk_hi ? 1u : 0u);
+    uint32_t tot = 0, n_ok = 0, my_off = 0, my_ci = 0;  // each group follows the earlier groups' entries
+#pragma unroll
+    for (uint32_t g = 0; g < kWarpGroups; ++g) {
+      const uint32_t kg = __shfl_sync(FULL, kk, int(g * kBfsLanes));
+      if (g * kBfsLanes == shift) {
+        my_off = tot;
+        my_ci = n_ok;
+      }
+      tot += kg;
+      n_ok += kg ? 1u : 0u;
+    }
     uint32_t off = 0, ci = 0;
     if (lane == 0 && n_ok) {
-      off = atomicAdd(&D.ctr->pool_used, kk_lo + (kWarpGroups > 1 ? kk_hi : 0u));
+      off = atomicAdd(&D.ctr->pool_used, tot);
       ci = atomicAdd(&D.ctr->n_cand, n_ok);
     }
-    off = __shfl_sync(FULL, off, 0);
-    ci = __shfl_sync(FULL, ci, 0);
-    if (shift) {  // the second group follows the first one's entries
-      off += kk_lo;
-      ci += kk_lo ? 1u : 0u;
-    }
+    off = __shfl_sync(FULL, off, 0) + my_off;
+    ci = __shfl_sync(FULL, ci, 0) + my_ci;
     ok = ok && off + K <= D.pool_cap;  // pool full: retry next round
     if (ok) {
       for (uint32_t k = gl; k < K; k += kBfsLanes) D.pool[off + k] = k < kBfsShared ? sq[k] : cav[k];
