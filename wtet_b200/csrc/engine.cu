@@ -12,12 +12,14 @@
 // equivalent to some sequential order.  The result is therefore the unique
 // SoS Delaunay triangulation, with no flip failures and nothing left to repair.
 //
-// Round structure (one insertion round over all clouds of a job; 10 kernels
+// Round structure (one insertion round over all clouds of a job; 9 kernels
 // replayed from a CUDA graph):
 //   k_activate    locate the new stratum's points (walk from the curve
 //                 predecessor's tet)
-//   k_vote        each uninserted point votes for its tet (64-bit atomicMax of
-//                 score | ~point, src/shaders/vote.wgsl semantics)
+//   (votes)       each uninserted point votes for its tet (64-bit atomicMax
+//                 of score | ~point, src/shaders/vote.wgsl semantics) when it
+//                 is located (k_activate) or relocated (k_relocate); a tet's
+//                 vote stays valid until the tet is retired
 //   k_cands       the winner of each tet becomes a candidate and pre-claims
 //                 its tet's neighbourhood with its claim key (with the
 //                 learned scheduler, k_cands_learned: the fused BF16 MLP sets
@@ -664,6 +666,52 @@ __global__ void k_init_clouds(const CloudInfo* ci, uint32_t nc, Dev D) {
 
 // ---------------------------------------------------------------- rounds ----
 
+// Vote score: larger = inserted first.  Circumcenter rule: depth of p inside
+// the circumsphere (f32 insphere, src/shaders/vote.wgsl:401-494 semantics);
+// centroid rule: inverse squared distance to the centroid.
+__device__ __forceinline__ float vote_score(const float4* pts, uint4 V, float4 q, int rule) {
+  float4 a = pts[V.x], b = pts[V.y], c = pts[V.z], d = pts[V.w];
+  if (rule == 1) {
+    float cx = 0.25f * (a.x + b.x + c.x + d.x) - q.x;
+    float cy = 0.25f * (a.y + b.y + c.y + d.y) - q.y;
+    float cz = 0.25f * (a.z + b.z + c.z + d.z) - q.z;
+    return 1.0f / (1e-30f + cx * cx + cy * cy + cz * cz);
+  }
+  float aex = a.x - q.x, aey = a.y - q.y, aez = a.z - q.z;
+  float bex = b.x - q.x, bey = b.y - q.y, bez = b.z - q.z;
+  float cex = c.x - q.x, cey = c.y - q.y, cez = c.z - q.z;
+  float dex = d.x - q.x, dey = d.y - q.y, dez = d.z - q.z;
+  float ab = aex * bey - bex * aey, bc = bex * cey - cex * bey, cd = cex * dey - dex * cey;
+  float da = dex * aey - aex * dey, ac = aex * cey - cex * aey, bd = bex * dey - dex * bey;
+  float abc = aez * bc - bez * ac + cez * ab, bcd = bez * cd - cez * bd + dez * bc;
+  float cda = cez * da + dez * ac + aez * cd, dab = dez * ab + aez * bd + bez * da;
+  float al = aex * aex + aey * aey + aez * aez, bl = bex * bex + bey * bey + bez * bez;
+  float cl = cex * cex + cey * cey + cez * cez, dl = dex * dex + dey * dey + dez * dez;
+  float det = (dl * abc - cl * dab) + (bl * cda - al * bcd);
+  float depth = -det;  // tets have Shewchuk orient3d < 0, so inside means det < 0
+  return (depth > 0.f && depth < 3.0e38f) ? depth : 0.f;
+}
+
+// The vote of uninserted point p for tet t: 64-bit atomicMax of (score, ~p),
+// so each tet's vote word names its point with the largest score (ties: the
+// smallest index).  A tet's points change only when it is retired, so its
+// vote word stays valid until then: points vote when they are located
+// (k_activate) or relocated (k_relocate), and k_write clears the word of
+// every slot it writes a new tet into.
+__device__ __forceinline__ void cast_vote(const Dev& D, uint32_t p, uint32_t t) {
+  if (t >= D.cap) {
+    atomicOr(&D.ctr->err, kErrGuard);
+    return;
+  }
+  const uint4 V = D.T[t].v;
+  if (V.x >= D.nv || V.y >= D.nv || V.z >= D.nv || V.w >= D.nv) {
+    atomicOr(&D.ctr->err, kErrGuard);
+    return;
+  }
+  const float sc = vote_score(D.pts, V, D.pts[p], D.rule);
+  atomicMax(&D.C[t].vote, ((unsigned long long)__float_as_uint(sc) << 32) | (unsigned long long)(~p));
+}
+
 // Locates the points of one stratum: walk from the tet of the point one
 // stride earlier on the Morton curve (a point of an earlier stratum: its tet
 // once inserted, else the tet that still contains it).  The located points are
@@ -704,58 +752,12 @@ __global__ void __launch_bounds__(512, WTET_RELOC_MINB) k_activate(Dev D) {
       }
     }
     if (t == NONE) t = D.centry[c];
-    D.loc[p] = walk_to(D, t, p, D.pts[p], steps);
+    const uint32_t lt = walk_to(D, t, p, D.pts[p], steps);
+    D.loc[p] = lt;
     D.bigflag[p] = 0;
+    cast_vote(D, p, lt);
   }
   if (steps) atomicAdd(&D.ctr->walk_steps, (unsigned long long)steps);
-}
-
-// Vote score: larger = inserted first.  Circumcenter rule: depth of p inside
-// the circumsphere (f32 insphere, src/shaders/vote.wgsl:401-494 semantics);
-// centroid rule: inverse squared distance to the centroid.
-__device__ __forceinline__ float vote_score(const float4* pts, uint4 V, float4 q, int rule) {
-  float4 a = pts[V.x], b = pts[V.y], c = pts[V.z], d = pts[V.w];
-  if (rule == 1) {
-    float cx = 0.25f * (a.x + b.x + c.x + d.x) - q.x;
-    float cy = 0.25f * (a.y + b.y + c.y + d.y) - q.y;
-    float cz = 0.25f * (a.z + b.z + c.z + d.z) - q.z;
-    return 1.0f / (1e-30f + cx * cx + cy * cy + cz * cz);
-  }
-  float aex = a.x - q.x, aey = a.y - q.y, aez = a.z - q.z;
-  float bex = b.x - q.x, bey = b.y - q.y, bez = b.z - q.z;
-  float cex = c.x - q.x, cey = c.y - q.y, cez = c.z - q.z;
-  float dex = d.x - q.x, dey = d.y - q.y, dez = d.z - q.z;
-  float ab = aex * bey - bex * aey, bc = bex * cey - cex * bey, cd = cex * dey - dex * cey;
-  float da = dex * aey - aex * dey, ac = aex * cey - cex * aey, bd = bex * dey - dex * bey;
-  float abc = aez * bc - bez * ac + cez * ab, bcd = bez * cd - cez * bd + dez * bc;
-  float cda = cez * da + dez * ac + aez * cd, dab = dez * ab + aez * bd + bez * da;
-  float al = aex * aex + aey * aey + aez * aez, bl = bex * bex + bey * bey + bez * bez;
-  float cl = cex * cex + cey * cey + cez * cez, dl = dex * dex + dey * dey + dez * dez;
-  float det = (dl * abc - cl * dab) + (bl * cda - al * bcd);
-  float depth = -det;  // tets have Shewchuk orient3d < 0, so inside means det < 0
-  return (depth > 0.f && depth < 3.0e38f) ? depth : 0.f;
-}
-
-__global__ void k_vote(Dev D) {
-  const RoundArgs R = load_round(D);
-  if (!R.live) return;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < R.n_active; i += gridDim.x * blockDim.x) {
-    uint32_t p = R.active[i];
-    if (D.bigflag[p] & kDup) continue;
-    uint32_t t = D.loc[p];
-    if (t >= D.cap) {
-      atomicOr(&D.ctr->err, kErrGuard);
-      continue;
-    }
-    uint4 V = D.T[t].v;
-    if (V.x >= D.nv || V.y >= D.nv || V.z >= D.nv || V.w >= D.nv) {
-      atomicOr(&D.ctr->err, kErrGuard);
-      continue;
-    }
-    float sc = vote_score(D.pts, V, D.pts[p], D.rule);
-    unsigned long long key = ((unsigned long long)__float_as_uint(sc) << 32) | (unsigned long long)(~p);
-    atomicMax(&D.C[t].vote, key);
-  }
 }
 
 // Prefix of the order buckets' start counts, in shared memory (sp has
@@ -1664,6 +1666,7 @@ __global__ void __launch_bounds__(128, WTET_WRITE_MINB) k_write(Dev D) {
     auto commit = [&](const uint4& nv, const uint4& nn, uint32_t sl, uint32_t outer, bool shared) {
       D.T[sl].v = nv;
       D.T[sl].n = nn;
+      D.C[sl].vote = 0ull;  // the new tet's points vote in k_relocate
       // Every vertex on the cavity boundary gets a live incident tet, so a
       // vertex's hint tet is alive whenever it is read (strata activation).
       for (int q = 0; q < 4; ++q)
@@ -1758,7 +1761,6 @@ __global__ void __launch_bounds__(512, WTET_RELOC_MINB) k_relocate(Dev D) {
         t = 0;
         L |= INS_BIT;
       }
-      D.C[t].vote = 0ull;
       if (!(L & INS_BIT)) {
         keep = true;
         if (D.bigflag[p] & kPending) D.bigflag[p] &= uint8_t(~kPending);
@@ -1776,7 +1778,11 @@ __global__ void __launch_bounds__(512, WTET_RELOC_MINB) k_relocate(Dev D) {
             if (q < D.nv && D.st2[q]) from = t;
           }
         }
-        if (from != NONE) D.loc[p] = walk_to(D, from, p, D.pts[p], steps);
+        if (from != NONE) {
+          const uint32_t lt = walk_to(D, from, p, D.pts[p], steps);
+          D.loc[p] = lt;
+          cast_vote(D, p, lt);
+        }
       }
     }
     uint32_t slot = warp_append(&D.ctr->n_next, keep);
@@ -2553,7 +2559,7 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   struct Grids {
     uint32_t act, vote, cand, candl, logf, bfs, res, sh, wr, rel;
   };
-  const Grids big{wave(k_activate, TB), wave(k_vote, TB),      wave(k_cands, TB),
+  const Grids big{wave(k_activate, TB), 0u,      wave(k_cands, TB),
                   vmode == 1 ? wave(k_cands_learned, 256) : 0u,
                   wave(k_log_features, TB), wave(k_bfs, 128), wave(k_resolve, 128), wave(k_shared, 128),
                   wave(k_write, 128),  wave(k_relocate, TB)};
@@ -2561,15 +2567,14 @@ JobResult run_job(const Job& job, uint32_t* d_out_t, uint32_t* d_out_a, uint64_t
   // blocks that exit at once costs more than their work, so those rounds
   // replay a graph with one block per SM.
   auto shrink = [](uint32_t g) { return std::min<uint32_t>(g, 148u); };
-  const Grids small{shrink(big.act), shrink(big.vote), shrink(big.cand), shrink(big.candl), shrink(big.logf),
+  const Grids small{shrink(big.act), 0u, shrink(big.cand), shrink(big.candl), shrink(big.logf),
                     shrink(big.bfs), shrink(big.res),  shrink(big.sh),   shrink(big.wr),    shrink(big.rel)};
-  const uint64_t kernels_per_round = 10 + (vmode == 2 ? 1 : 0);
+  const uint64_t kernels_per_round = 9 + (vmode == 2 ? 1 : 0);
 
   // One round: k_end also starts the next round (k_begin starts the first).
   // `learned`: the learned scheduler's candidate kernel.
   auto enqueue_round = [&](const Grids& G, bool learned) {
     k_activate<<<G.act, TB, 0, s>>>(D);
-    k_vote<<<G.vote, TB, 0, s>>>(D);
     if (learned) k_cands_learned<<<G.candl, 256, 0, s>>>(D);
     else k_cands<<<G.cand, TB, 0, s>>>(D);
     if (vmode == 2) k_log_features<<<G.logf, TB, 0, s>>>(D);
