@@ -463,48 +463,57 @@ def variants(wt, args, golden):
 
     L = wt._core.load()
     stream = torch.cuda.current_stream()
-    reps = 3
+    reps = 5
     out = {}
 
-    def measure(pts, vote, gname):
+    def compare(pts, gname):
+        """Plain and learned on the same cloud: one warm-up each, then reps
+        runs of each, alternating, so that a slow period of the shared host
+        or GPU affects both; median device time of each."""
         n = len(pts)
         d_pts = torch.from_numpy(pts).cuda()
         cap = int(L.wtet_max_tets(n))
-        d_t = torch.empty((cap, 4), dtype=torch.int32, device="cuda")
-        d_a = torch.empty((cap, 4), dtype=torch.int32, device="cuda")
-        cfg = wt.Config(vote=vote)._c()
-        device_run(wt, L, d_pts, n, cfg, d_t, d_a, cap, stream)
-        runs = [device_run(wt, L, d_pts, n, cfg, d_t, d_a, cap, stream) for _ in range(reps)]
-        m, st = runs[-1]
-        dig = device_digest(wt, d_t, d_a, m, n)
-        ms = float(np.median([r[1].device_ms for r in runs]))
-        rec = {"mpts": round(n / (ms * 1e3), 3), "device_ms": round(ms, 2), "rounds": int(st.rounds),
-               "vote_winners": int(st.vote_winners), "cavity_searches": int(st.candidates),
-               "same_as_oracle": bool(gname in golden and dig == golden[gname]["sha256"])}
-        del d_t, d_a, d_pts
+        votes = ("plain", "learned")
+        bufs = {v: (torch.empty((cap, 4), dtype=torch.int32, device="cuda"),
+                    torch.empty((cap, 4), dtype=torch.int32, device="cuda")) for v in votes}
+        cfgs = {v: wt.Config(vote=v)._c() for v in votes}
+        for v in votes:
+            device_run(wt, L, d_pts, n, cfgs[v], *bufs[v], cap, stream)
+        runs = {v: [] for v in votes}
+        for _ in range(reps):
+            for v in votes:
+                runs[v].append(device_run(wt, L, d_pts, n, cfgs[v], *bufs[v], cap, stream))
+        recs = {}
+        for v in votes:
+            m, st = runs[v][-1]
+            dig = device_digest(wt, *bufs[v], m, n)
+            ms = float(np.median([r[1].device_ms for r in runs[v]]))
+            recs[v] = {"mpts": round(n / (ms * 1e3), 3), "device_ms": round(ms, 2), "rounds": int(st.rounds),
+                       "vote_winners": int(st.vote_winners), "cavity_searches": int(st.candidates),
+                       "same_as_oracle": bool(gname in golden and dig == golden[gname]["sha256"])}
+        del bufs, d_pts
         torch.cuda.empty_cache()
-        return rec
+        return recs
 
     seeds = []
     for seed in range(101, 106):
-        pts = syn.mixture(8_000_000, seed)
         rec = {"seed": seed}
-        for vote in ("plain", "learned"):
-            for k, v in measure(pts, vote, f"mixture8M_s{seed}").items():
+        for vote, r in compare(syn.mixture(8_000_000, seed), f"mixture8M_s{seed}").items():
+            for k, v in r.items():
                 rec[f"{vote}_{k}"] = v
         seeds.append(rec)
     out["learned"] = {
         "workload": "8,000,000-point mixture clouds, seeds 101-105",
+        "how": f"per seed: one warm-up each, then {reps} runs of each scheduler alternating; median device time",
         "per_seed": seeds,
         "plain_mpts_mean": round(float(np.mean([r["plain_mpts"] for r in seeds])), 3),
         "learned_mpts_mean": round(float(np.mean([r["learned_mpts"] for r in seeds])), 3),
         "learned_faster_on": sum(r["learned_mpts"] > r["plain_mpts"] for r in seeds),
         "all_same_as_oracle": all(r["plain_same_as_oracle"] and r["learned_same_as_oracle"] for r in seeds),
     }
-    lat = syn.lattice(128)
     out["learned_lattice"] = {"workload": "lattice2M",
-                              **{f"{v}_{k}": x for v in ("plain", "learned")
-                                 for k, x in measure(lat, v, "lattice128").items()}}
+                              **{f"{v}_{k}": x for v, r in compare(syn.lattice(128), "lattice128").items()
+                                 for k, x in r.items()}}
     clouds = make_workload("batched")
     n = sum(len(c) for c in clouds)
     wt.delaunay_batched(clouds)
