@@ -398,10 +398,11 @@ def run_gpu(args):
 # launch per capture) times that kernel's total time in the time-only launch
 # list of one 8M triangulation.  It describes the kernels it was measured on
 # and must be captured again when they change.
-TRAFFIC: dict = {"mixture8M": 311.8e9}
+TRAFFIC: dict = {"mixture8M": 366.7e9}
 TRAFFIC_SOURCE = ("estimate: sum over k_bfs, k_shared, k_write, k_cands, k_vote, k_relocate, k_activate of "
                   "(DRAM bytes per us of one bulk-round launch on the 1M mixture, ncu) x (the kernel's total time "
-                  "in the 8M launch list, ncu); early rounds fit in L2, so this over-counts them")
+                  "in the 8M launch list, ncu); early rounds fit in L2, so this over-counts them; two captures of "
+                  "different bulk rounds gave 312 and 367 GB")
 
 WORKLOADS = {
     "mixture8M": "8,000,000 points: 60% uniform [0,1]^3, 30% Gaussian ball (0.5, sigma 0.1), "
