@@ -245,6 +245,8 @@ class Config:
     ``block_size``, ``rounds_per_graph``, ``overlap_shift``,
     ``candidate_filter`` and ``pool_factor`` are performance knobs (0 = the
     autotuner's value for the job's size, see wtet_b200.autotune);
+    ``learned_gate`` bounds the rounds the learned scheduler serves (rounds
+    that may see at most learned_gate x 1024 uninserted points; 0 = 2048);
     ``initial_capacity`` sets the initial tet slots per point in eighths (0 =
     9 per point; smaller values exercise the in-place growth of the tet
     arrays).  No option changes the resulting triangulation."""
