@@ -85,9 +85,6 @@
 #ifndef WTET_SMALL_ROUND_POINTS
 #define WTET_SMALL_ROUND_POINTS 32768
 #endif
-#ifndef WTET_SHARED_TEST
-#define WTET_SHARED_TEST o4d_sos_call
-#endif
 #ifndef WTET_RELOC_MINB
 #define WTET_RELOC_MINB 1
 #endif
@@ -1388,7 +1385,7 @@ __global__ void __launch_bounds__(128, WTET_SHARED_MINB) k_shared(Dev D) {
               const uint4 V = D.T[c].v;
               const uint32_t w0 = f == 0 ? p : V.x, w1 = f == 1 ? p : V.y, w2 = f == 2 ? p : V.z,
                              w3 = f == 3 ? p : V.w;
-              if (WTET_SHARED_TEST(D.pts[w0], D.pts[w1], D.pts[w2], D.pts[w3], D.pts[q], w0, w1, w2, w3, q, D.sos,
+              if (o4d_sos_call(D.pts[w0], D.pts[w1], D.pts[w2], D.pts[w3], D.pts[q], w0, w1, w2, w3, q, D.sos,
                             &D.ctr->err) < 0)
                 bad = true;
             }
