@@ -571,12 +571,25 @@ def host_cpu():
     return f"{os.cpu_count()} cpus"
 
 
+def host_memory_available():
+    """Bytes of host memory available now (MemAvailable), or None."""
+    try:
+        with open("/proc/meminfo") as f:
+            for ln in f:
+                if ln.startswith("MemAvailable:"):
+                    return int(ln.split()[1]) * 1024
+    except Exception:
+        pass
+    return None
+
+
 def run_reference(args):
     """CPU reference arm: the reference's CPU algorithm (the oracle port of
     src/phase2.rs:383-606 with walk point location; the Rust/wgpu reference
-    cannot be built or run here) on every host core.  A step is one complete
-    triangulation of the same workload as the GPU arm; the threads take steps
-    from a queue (W untimed warm-up steps first, then exactly K timed steps)."""
+    cannot be built or run here) on every host core (as many at once as host
+    memory holds).  A step is one complete triangulation of the same workload
+    as the GPU arm; the threads take steps from a queue (W untimed warm-up
+    steps first, then exactly K timed steps)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -587,6 +600,14 @@ def run_reference(args):
     oracle.build()
     clouds = make_workload(args.workload)
     threads = max(1, os.cpu_count() or 1)
+    # Concurrent triangulations are bounded by host memory as well: one
+    # oracle triangulation holds about 540 B per point at its peak (4.3 GB
+    # for the 8M mixture); 600 B per point and 80% of the available memory
+    # leave a margin.
+    avail = host_memory_available()
+    if avail:
+        per_run = 600 * max(len(c) for c in clouds)
+        threads = max(1, min(threads, int(0.8 * avail) // per_run))
 
     def one_step():
         for c in clouds:
