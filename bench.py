@@ -399,7 +399,7 @@ def run_gpu(args):
 # list of one 8M triangulation.  It describes the kernels it was measured on
 # and must be captured again when they change.
 TRAFFIC: dict = {"mixture8M": 366.7e9}
-TRAFFIC_SOURCE = ("estimate: sum over k_bfs, k_shared, k_write, k_cands, k_vote, k_relocate, k_activate of "
+TRAFFIC_SOURCE = ("estimate: sum over k_bfs, k_shared, k_write, k_cands, k_relocate, k_activate of "
                   "(DRAM bytes per us of one bulk-round launch on the 1M mixture, ncu) x (the kernel's total time "
                   "in the 8M launch list, ncu); early rounds fit in L2, so this over-counts them; two captures of "
                   "different bulk rounds gave 312 and 367 GB")
